@@ -1,0 +1,224 @@
+"""B200-native solver for the per-step residual-and-update loop of the 2-D unstructured
+cell-centred finite-volume Euler solver of Hasti-Jalal-Aldeen/CFD_Optimisations.
+
+The compute path is libhcfd_gpu.so (hand-written CUDA for sm_100a behind the C ABI of
+include/hcfd_gpu.h).  This package is its Python binding:
+
+* ``Mesh``    — .hmsh reader/writer, wedge generator, renumbering (the reference's Mesh,
+                includes/Mesh.hpp).
+* ``Solver``  — one mesh on one GPU: gather_bcs / initialise / step / download.
+* ``GPU``     — classes with the names and signatures of the reference's Base layout
+                (Domain, GaussGreen, Limiter, Flux, Euler, Writer), so a driver written
+                against the reference swaps namespaces.
+* ``arena``   — many meshes packed into one device arena (batched and served solves).
+
+Nothing here computes on the CPU: without the native library or a CUDA device every
+solver call raises.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+
+from . import native as _n
+from .native import (FIXED_DT, GLOBAL_CFL, LOCAL_CFL, FP32, FP64, LIMITER_BJ, LIMITER_VENKAT,
+                     NUMBER_MORTON, NUMBER_NATURAL, NUMBER_RANDOM, NUMBER_RCM, SUBINLET, SUBOUTLET,
+                     SUPINLET, SUPOUTLET, SYMMETRY, WALL, HcfdError)
+
+__all__ = ["Mesh", "Solver", "HcfdError", "FIXED_DT", "GLOBAL_CFL", "LOCAL_CFL", "FP32", "FP64",
+           "LIMITER_BJ", "LIMITER_VENKAT", "NUMBER_NATURAL", "NUMBER_RANDOM", "NUMBER_RCM",
+           "NUMBER_MORTON", "SYMMETRY", "WALL", "SUPINLET", "SUBINLET", "SUPOUTLET", "SUBOUTLET",
+           "write_hsln", "wedge_case"]
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(ct.POINTER(ct.c_int))
+
+
+class Mesh:
+    """A host mesh owned by the native library (the reference's Mesh, src/Mesh.cpp)."""
+
+    def __init__(self, path: str | None = None, _handle=None):
+        L = _n.lib()
+        if _handle is not None:
+            self._h = _handle
+        else:
+            h = ct.c_void_p()
+            _n.check(L.hcfd_mesh_load(path.encode(), ct.byref(h)))
+            self._h = h
+
+    @classmethod
+    def wedge(cls, nx: int, ny: int, theta_deg: float = 15.0, jitter: float = 0.15, seed: int = 1234,
+              numbering: int = NUMBER_RANDOM, length: float = 3.0, height: float = 1.5,
+              x_ramp: float = 0.5) -> "Mesh":
+        """Triangulated supersonic wedge (see hcfd_mesh_generate_wedge)."""
+        spec = _n.WedgeSpec(nx, ny, length, height, x_ramp, theta_deg, jitter, seed, numbering)
+        h = ct.c_void_p()
+        _n.check(_n.lib().hcfd_mesh_generate_wedge(ct.byref(spec), ct.byref(h)))
+        return cls(_handle=h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _n.lib().hcfd_mesh_free(h)
+            self._h = None
+
+    def renumber(self, numbering: int, seed: int = 0) -> "Mesh":
+        _n.check(_n.lib().hcfd_mesh_renumber(self._h, numbering, seed))
+        return self
+
+    def write(self, path: str) -> None:
+        _n.check(_n.lib().hcfd_mesh_write(self._h, path.encode()))
+
+    def view(self) -> _n.MeshView:
+        v = _n.MeshView()
+        _n.check(_n.lib().hcfd_mesh_view_of(self._h, ct.byref(v)))
+        return v
+
+    def arrays(self) -> dict:
+        """Copies of the mesh arrays, keyed like the reference's Mesh members."""
+        v = self.view()
+
+        def take(ptr, n, dt):
+            if not ptr or n == 0:
+                return None
+            return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True)
+
+        cn_off = take(v.cn_off, v.Nc + 1, np.int32)
+        d = dict(dim=v.dim, Nn=v.Nn, Ncol=v.Ncol, NBCcol=v.NBCcol, Nc=v.Nc, Nf=v.Nf,
+                 coltag=take(v.coltag, v.Ncol, np.int32), coloff=take(v.coloff, v.Ncol + 1, np.int32),
+                 nodes=take(v.nodes, 2 * v.Nn, np.float64), fn_con=take(v.fn_con, 2 * v.Nf, np.int32),
+                 fc_con=take(v.fc_con, 2 * v.Nf, np.int32), cn_off=cn_off,
+                 cn_con=take(v.cn_con, int(cn_off[-1]), np.int32))
+        if v.cc_off:
+            cc_off = take(v.cc_off, v.Nc + 1, np.int32)
+            d["cc_off"] = cc_off
+            d["cc_con"] = take(v.cc_con, int(cc_off[-1]), np.int32)
+        cfo, cfc = _n._ip(), _n._ip()
+        _n.check(_n.lib().hcfd_mesh_cf(self._h, ct.byref(cfo), ct.byref(cfc)))
+        d["cf_off"] = take(cfo, v.Nc + 1, np.int32)
+        d["cf_con"] = take(cfc, int(d["cf_off"][-1]), np.int32)
+        d["pnames"] = []
+        for k in range(64):
+            s = _n.lib().hcfd_mesh_pname(self._h, k)
+            if s is None:
+                break
+            d["pnames"].append(s.decode())
+        return d
+
+    @property
+    def Nc(self):
+        return self.view().Nc
+
+    @property
+    def Nf(self):
+        return self.view().Nf
+
+
+class Solver:
+    """One mesh on one GPU (include/hcfd_gpu.h, hcfd_gpu_*)."""
+
+    def __init__(self, mesh: Mesh, gma: float = 1.4, limiter: int = LIMITER_BJ, venkat_K: float = 5.0,
+                 precision: int = FP64, block: int = 0):
+        self._mesh = mesh
+        v = mesh.view()
+        p = _n.Params(gma, limiter, venkat_K, precision, block)
+        h = ct.c_void_p()
+        _n.check(_n.lib().hcfd_gpu_create(ct.byref(v), ct.byref(p), ct.byref(h)))
+        self._h = h
+        self.gma = gma
+        self.precision = precision
+        Nc, Nf, Nr, W = ct.c_int(), ct.c_int(), ct.c_int(), ct.c_int()
+        _n.check(_n.lib().hcfd_gpu_info(h, ct.byref(Nc), ct.byref(Nf), ct.byref(Nr), ct.byref(W)))
+        self.Nc, self.Nf, self.Nreal, self.slots = Nc.value, Nf.value, Nr.value, W.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _n.lib().hcfd_gpu_destroy(h)
+            self._h = None
+
+    def gather_bcs(self, bcmap, qbc) -> None:
+        bm = np.ascontiguousarray(bcmap, dtype=np.int32)
+        q = np.ascontiguousarray(qbc, dtype=np.float64).reshape(-1)
+        _n.check(_n.lib().hcfd_gpu_gather_bcs(self._h, _iptr(bm), len(bm), _dptr(q)))
+
+    def initialise(self, qic) -> None:
+        q = np.ascontiguousarray(qic, dtype=np.float64)
+        _n.check(_n.lib().hcfd_gpu_initialise(self._h, _dptr(q)))
+
+    def step(self, nsteps: int = 1, mode: int = FIXED_DT, dt_or_cfl: float = 1e-3, wait: bool = True):
+        """Advances nsteps steps; returns the step statistics when wait is true."""
+        st = _n.StepStats() if wait else None
+        _n.check(_n.lib().hcfd_gpu_step(self._h, nsteps, mode, dt_or_cfl, ct.byref(st) if wait else None))
+        return self._stats_dict(st) if wait else None
+
+    @staticmethod
+    def _stats_dict(st):
+        return dict(dt=st.dt, res_l2=st.res_l2, res_first=st.res_first, steps=st.steps,
+                    nonfinite=bool(st.nonfinite))
+
+    def stats(self) -> dict:
+        st = _n.StepStats()
+        _n.check(_n.lib().hcfd_gpu_stats(self._h, ct.byref(st)))
+        return self._stats_dict(st)
+
+    def sync(self) -> None:
+        _n.check(_n.lib().hcfd_gpu_sync(self._h))
+
+    def download(self, prims: bool = False, out: np.ndarray | None = None) -> np.ndarray:
+        out = np.empty((4, self.Nc)) if out is None else out
+        ptrs = (ct.POINTER(ct.c_double) * 4)(*[_dptr(out[v]) for v in range(4)])
+        _n.check(_n.lib().hcfd_gpu_download(self._h, 1 if prims else 0, ptrs))
+        return out
+
+    def U(self) -> np.ndarray:
+        return self.download(False)
+
+    def Q(self) -> np.ndarray:
+        return self.download(True)
+
+    def upload(self, U: np.ndarray) -> None:
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(4, self.Nc)
+        ptrs = (ct.POINTER(ct.c_double) * 4)(*[_dptr(U[v]) for v in range(4)])
+        _n.check(_n.lib().hcfd_gpu_upload(self._h, ptrs))
+
+    def wall_cp(self, colour: int, rho_inf: float, p_inf: float, speed_inf: float) -> np.ndarray:
+        out = np.empty(self.Nf)
+        n = ct.c_int()
+        _n.check(_n.lib().hcfd_gpu_wall_cp(self._h, colour, rho_inf, p_inf, speed_inf, _dptr(out), ct.byref(n)))
+        return out[:n.value].copy()
+
+    def profile(self, enable: bool) -> None:
+        _n.check(_n.lib().hcfd_gpu_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        m1, m2 = ct.c_double(), ct.c_double()
+        n1, n2 = ct.c_longlong(), ct.c_longlong()
+        _n.check(_n.lib().hcfd_gpu_profile_read(self._h, ct.byref(m1), ct.byref(n1), ct.byref(m2), ct.byref(n2)))
+        return dict(ms_pass1=m1.value, n_pass1=n1.value, ms_pass2=m2.value, n_pass2=n2.value)
+
+
+def write_hsln(path: str, arrs, varnames=("Density", "Velocity_X", "Velocity_Y", "Pressure")) -> None:
+    """Writer::write_soln's file format (src/Writer.cpp:22-39)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
+    nv, Nc = len(arrs), arrs[0].shape[0]
+    names = (ct.c_char_p * nv)(*[s.encode() for s in varnames[:nv]])
+    ptrs = (ct.POINTER(ct.c_double) * nv)(*[_dptr(a) for a in arrs])
+    _n.check(_n.lib().hcfd_write_hsln(path.encode(), nv, names, Nc, ptrs))
+
+
+def wedge_case(mach: float = 2.5, rho: float = 1.4, p: float = 1.0, gma: float = 1.4):
+    """Boundary map and states of the supersonic-wedge family: colour tags 1 upper / 2 lower
+    slip walls (SYMMETRY), 3 inlet SUPINLET, 4 outlet SUPOUTLET (src/Test.cpp:64); uniform
+    freestream (rho, u = M a, 0, p) as the initial and boundary state."""
+    a = (gma * p / rho) ** 0.5
+    q = np.array([rho, mach * a, 0.0, p])
+    bcmap = np.array([SYMMETRY, SYMMETRY, SYMMETRY, SUPINLET, SUPOUTLET], dtype=np.int32)
+    qbc = np.tile(q, (4, 1))
+    return bcmap, qbc, q

@@ -1,0 +1,35 @@
+// Internal declarations shared by the host and device translation units of libhcfd_gpu.
+#pragma once
+#include "hcfd_gpu.h"
+
+#include <string>
+#include <vector>
+
+namespace hcfd {
+
+// Thread-local text behind hcfd_last_error(); every failing entry point sets it.
+int fail(int code, const std::string& msg);
+void clear_error();
+
+}  // namespace hcfd
+
+// Host mesh: the public arrays of the reference's Mesh (includes/Mesh.hpp:4-22) plus the
+// cell->face table it derives (src/Mesh.cpp:88-117) and the c_ctypes the Python importer
+// writes (interface/Mesh.py:463).
+struct hcfd_mesh {
+    int dim = 2, Nn = 0, Ncol = 0, NBCcol = 0, Nc = 0, Nf = 0;
+    std::vector<std::string> pnames;
+    std::vector<int> coltag, coloff;
+    std::vector<double> nodes;
+    std::vector<int> fn_con, fc_con, cn_off, cn_con, cc_off, cc_con, c_ctypes;
+    std::vector<int> cf_off, cf_con;
+};
+
+namespace hcfd {
+// Checks index ranges and the colour/ghost conventions of a mesh view.  Returns HCFD_OK or
+// HCFD_EINVAL with the reason recorded.
+int validate_view(const hcfd_mesh_view& v);
+// Builds cf_off/cf_con exactly as Mesh::compute_cf_con does (faces of each cell in
+// increasing face index).
+void build_cf(int Nc, int Nf, const int* fc_con, std::vector<int>& cf_off, std::vector<int>& cf_con);
+}  // namespace hcfd

@@ -1,0 +1,480 @@
+// Solver handle of the B200 solver: device memory, the per-handle stream, launches of the
+// step kernels and the C ABI of include/hcfd_gpu.h for one mesh.
+#include "hcfd_internal.hpp"
+#include "hcfd_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <type_traits>
+#include <string>
+#include <vector>
+
+using hcfd::fail;
+
+namespace {
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(HCFD_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+template <class P>
+int dalloc(P** p, size_t n) {
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**) p, n * sizeof(P));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(e == cudaErrorMemoryAllocation ? HCFD_ENOMEM : HCFD_ECUDA,
+                    std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return HCFD_OK;
+}
+
+inline int nblk(long long n, int b) { return (int) ((n + b - 1) / b); }
+
+// Primitive -> conservative, BoundaryCondition::init (src/Base/BoundaryConditions/Base.cpp:18-22).
+void prim_to_cons(const double* q, double gma, double* u) {
+    u[0] = q[0];
+    for (int v = 1; v < 4; v++) u[v] = q[0] * q[v];
+    u[3] = q[3] / (gma - 1) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2]);
+}
+
+}  // namespace
+
+struct hcfd_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    hcfd_params prm{};
+    int Nc = 0, Nf = 0, Nn = 0, Ncol = 0, NBC = 0, F_BC = 0, Nreal = 0, W = 0;
+    std::vector<int> coloff, coltag;
+    bool bcs_set = false, initialised = false;
+    hcfd::BCTable bc{};
+    // device buffers
+    int* d_fc = nullptr;                 // fc_con [2 Nf]
+    int2* d_slot = nullptr;              // [W][Nc]
+    void* d_geo = nullptr;               // FaceGeo<T> [Nf]
+    hcfd::FaceGeo<double>* d_geo64 = nullptr;
+    void* d_iv = nullptr;                // T [Nc]
+    double* d_iv64 = nullptr;
+    void* d_U[2] = {nullptr, nullptr};   // Cell4<T> [Nc]
+    void* d_phiG = nullptr;              // Grad8<T> [Nc]
+    double* d_io = nullptr;              // 4 Nc doubles staging for upload/download
+    double* d_cp = nullptr;              // Nf doubles for the wall Cp
+    unsigned long long* d_dtmin = nullptr;   // [2]
+    double* d_partial = nullptr;
+    unsigned int* d_counter = nullptr;
+    hcfd::StepStats* d_stats = nullptr;
+    int cur = 0;                         // which of d_U holds the state
+    int block = 256;
+    // profiling
+    bool prof = false;
+    std::vector<cudaEvent_t> ev1, ev2;   // start/stop pairs per launch
+    double ms1 = 0, ms2 = 0;
+    long long n1 = 0, n2 = 0;
+
+    bool fp32() const { return prm.precision == HCFD_FP32; }
+};
+
+namespace {
+
+void free_all(hcfd_solver* s) {
+    if (!s) return;
+    if (s->device >= 0) cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto e : s->ev1) cudaEventDestroy(e);
+    for (auto e : s->ev2) cudaEventDestroy(e);
+    void* ptrs[] = {s->d_fc, s->d_slot, s->d_geo, s->d_geo64, s->d_iv, s->d_iv64, s->d_U[0], s->d_U[1],
+                    s->d_phiG, s->d_io, s->d_cp, s->d_dtmin, s->d_partial, s->d_counter, s->d_stats};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+template <class T>
+hcfd::StepArgs<T> step_args(hcfd_solver* s, int time_mode, double dt_or_cfl) {
+    hcfd::StepArgs<T> a;
+    a.U = (const hcfd::Cell4<T>*) s->d_U[s->cur];
+    a.Unew = (hcfd::Cell4<T>*) s->d_U[1 - s->cur];
+    a.phiG = (hcfd::Grad8<T>*) s->d_phiG;
+    a.geo = (const hcfd::FaceGeo<T>*) s->d_geo;
+    a.slot = s->d_slot;
+    a.iv = (const T*) s->d_iv;
+    a.dtmin = s->d_dtmin + s->cur;
+    a.dtmin_next = s->d_dtmin + (1 - s->cur);
+    a.partial = s->d_partial;
+    a.counter = s->d_counter;
+    a.stats = s->d_stats;
+    a.Nc = s->Nc;
+    a.F_BC = s->F_BC;
+    a.limiter = s->prm.limiter;
+    a.time_mode = time_mode;
+    a.gma = T(s->prm.gma);
+    a.venkat_K = T(s->prm.venkat_K);
+    a.dt_or_cfl = dt_or_cfl;
+    a.bc = s->bc;
+    return a;
+}
+
+template <class T, int W>
+int launch_step(hcfd_solver* s, int time_mode, double dt_or_cfl) {
+    const int grid = nblk(s->Nc, s->block);
+    hcfd::StepArgs<T> a = step_args<T>(s, time_mode, dt_or_cfl);
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+    if (s->prof) {
+        CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1)); CK(cudaEventCreate(&e2)); CK(cudaEventCreate(&e3));
+        CK(cudaEventRecord(e0, s->stream));
+    }
+    hcfd::pass1_kernel<T, W><<<grid, s->block, 0, s->stream>>>(a);
+    if (s->prof) { CK(cudaEventRecord(e1, s->stream)); CK(cudaEventRecord(e2, s->stream)); }
+    hcfd::pass2_kernel<T, W, std::is_same<T, float>::value><<<grid, s->block, 0, s->stream>>>(a);
+    if (s->prof) {
+        CK(cudaEventRecord(e3, s->stream));
+        s->ev1.push_back(e0); s->ev1.push_back(e1);
+        s->ev2.push_back(e2); s->ev2.push_back(e3);
+    }
+    CK(cudaGetLastError());
+    s->cur = 1 - s->cur;
+    return HCFD_OK;
+}
+
+template <class T>
+int launch_step_w(hcfd_solver* s, int time_mode, double dt_or_cfl) {
+    switch (s->W) {
+    case 3: return launch_step<T, 3>(s, time_mode, dt_or_cfl);
+    case 4: return launch_step<T, 4>(s, time_mode, dt_or_cfl);
+    default: return launch_step<T, 8>(s, time_mode, dt_or_cfl);
+    }
+}
+
+template <class T>
+int refresh_ghosts(hcfd_solver* s) {
+    const int nbf = s->Nf - s->F_BC;
+    if (nbf > 0)
+        hcfd::bc_cells_kernel<T><<<nblk(nbf, 256), 256, 0, s->stream>>>(
+            s->Nf, s->F_BC, s->d_fc, (const hcfd::FaceGeo<T>*) s->d_geo, (hcfd::Cell4<T>*) s->d_U[s->cur],
+            T(s->prm.gma), s->bc);
+    CK(cudaGetLastError());
+    return HCFD_OK;
+}
+
+int check_handle(hcfd_solver* s) {
+    if (!s) return fail(HCFD_EINVAL, "null solver handle");
+    CK(cudaSetDevice(s->device));
+    return HCFD_OK;
+}
+
+int read_stats(hcfd_solver* s, hcfd_step_stats* out) {
+    hcfd::StepStats st;
+    CK(cudaMemcpyAsync(&st, s->d_stats, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (out) {
+        out->dt = st.dt_last;
+        out->res_l2 = s->Nreal > 0 ? std::sqrt(st.res2_last / s->Nreal) : 0.0;
+        out->res_first = s->Nreal > 0 ? std::sqrt(st.res2_first / s->Nreal) : 0.0;
+        out->steps = st.steps;
+        out->nonfinite = st.nonfinite;
+    }
+    return st.nonfinite ? fail(HCFD_ENONFINITE, "a step produced a NaN or Inf") : HCFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solver** out) {
+    hcfd::clear_error();
+    if (!mv || !out) return fail(HCFD_EINVAL, "gpu_create: null argument");
+    *out = nullptr;
+    int rc = hcfd::validate_view(*mv);
+    if (rc != HCFD_OK) return rc;
+    hcfd_params p{1.4, HCFD_LIMITER_BJ, 5.0, HCFD_FP64, 0};
+    if (prm) p = *prm;
+    if (!(p.gma > 1.0) || (p.limiter != HCFD_LIMITER_BJ && p.limiter != HCFD_LIMITER_VENKAT) ||
+        (p.precision != HCFD_FP64 && p.precision != HCFD_FP32) || p.block < 0 || p.block > 1024 || (p.block % 32))
+        return fail(HCFD_EINVAL, "gpu_create: bad parameters");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(HCFD_ECUDA, "gpu_create: no CUDA device");
+
+    auto s = std::make_unique<hcfd_solver>();
+    CK(cudaGetDevice(&s->device));
+    s->prm = p;
+    s->block = p.block ? p.block : 256;
+    s->Nc = mv->Nc; s->Nf = mv->Nf; s->Nn = mv->Nn; s->Ncol = mv->Ncol; s->NBC = mv->NBCcol;
+    s->coloff.assign(mv->coloff, mv->coloff + mv->Ncol + 1);
+    s->coltag.assign(mv->coltag, mv->coltag + mv->Ncol);
+    s->F_BC = s->coloff[s->Ncol - s->NBC];
+    if (s->NBC > hcfd::MAXBC) return fail(HCFD_EINVAL, "gpu_create: more than 16 boundary colours");
+
+    // Cell -> face slots (ELL, slot-major) from the reference's CSR table: faces of each
+    // real cell in increasing face index; ghost cells get no slots.
+    std::vector<int> cf_off, cf_con;
+    hcfd::build_cf(s->Nc, s->Nf, mv->fc_con, cf_off, cf_con);
+    std::vector<char> ghost(s->Nc, 0);
+    for (int f = s->F_BC; f < s->Nf; f++) ghost[mv->fc_con[2 * f + 1]] = 1;
+    int maxdeg = 0;
+    for (int c = 0; c < s->Nc; c++) {
+        if (ghost[c]) continue;
+        s->Nreal++;
+        maxdeg = std::max(maxdeg, cf_off[c + 1] - cf_off[c]);
+    }
+    if (maxdeg > 8) return fail(HCFD_EINVAL, "gpu_create: a cell has more than 8 faces");
+    s->W = maxdeg <= 3 ? 3 : maxdeg <= 4 ? 4 : 8;
+    std::vector<int2> slot((size_t) s->W * s->Nc, make_int2(-1, -1));
+    for (int c = 0; c < s->Nc; c++) {
+        if (ghost[c]) continue;
+        int k = 0;
+        for (int j = cf_off[c]; j < cf_off[c + 1]; j++, k++) {
+            const int f = cf_con[j];
+            const int L = mv->fc_con[2 * f], R = mv->fc_con[2 * f + 1];
+            slot[(size_t) k * s->Nc + c] = (L == c) ? make_int2(f, R) : make_int2(~f, L);
+        }
+    }
+
+    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    hcfd_solver* h = s.get();
+    auto bail = [&](int code) { free_all(h); s.release(); delete h; return code; };
+    const bool f32 = p.precision == HCFD_FP32;
+    const size_t tsz = f32 ? sizeof(float) : sizeof(double);
+    int* d_fn = nullptr; int* d_cnoff = nullptr; int* d_cncon = nullptr; int* d_cfoff = nullptr; int* d_cfcon = nullptr;
+    double* d_nodes = nullptr; double* d_xc = nullptr;
+    auto free_tmp = [&]() {
+        cudaStreamSynchronize(h->stream);
+        void* t[] = {d_fn, d_cnoff, d_cncon, d_cfoff, d_cfcon, d_nodes, d_xc};
+        for (void* q : t) if (q) cudaFree(q);
+    };
+    int ncn = mv->cn_off[mv->Nc];
+    if ((rc = dalloc(&h->d_fc, 2 * (size_t) h->Nf)) || (rc = dalloc(&h->d_slot, slot.size())) ||
+        (rc = dalloc((char**) &h->d_geo, tsz * 8 * h->Nf)) || (rc = dalloc(&h->d_geo64, h->Nf)) ||
+        (rc = dalloc((char**) &h->d_iv, tsz * h->Nc)) || (rc = dalloc(&h->d_iv64, h->Nc)) ||
+        (rc = dalloc((char**) &h->d_U[0], tsz * 4 * h->Nc)) || (rc = dalloc((char**) &h->d_U[1], tsz * 4 * h->Nc)) ||
+        (rc = dalloc((char**) &h->d_phiG, tsz * 8 * h->Nc)) || (rc = dalloc(&h->d_io, 4 * (size_t) h->Nc)) ||
+        (rc = dalloc(&h->d_cp, h->Nf)) || (rc = dalloc(&h->d_dtmin, 2)) ||
+        (rc = dalloc(&h->d_partial, nblk(h->Nc, h->block))) || (rc = dalloc(&h->d_counter, 1)) ||
+        (rc = dalloc(&h->d_stats, 1)) || (rc = dalloc(&d_fn, 2 * (size_t) h->Nf)) ||
+        (rc = dalloc(&d_cnoff, h->Nc + 1)) || (rc = dalloc(&d_cncon, ncn)) || (rc = dalloc(&d_cfoff, h->Nc + 1)) ||
+        (rc = dalloc(&d_cfcon, cf_con.size())) || (rc = dalloc(&d_nodes, 2 * (size_t) h->Nn)) ||
+        (rc = dalloc(&d_xc, 2 * (size_t) h->Nc))) {
+        free_tmp();
+        return bail(rc);
+    }
+    cudaStream_t st = h->stream;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    };
+    cudaError_t ce = cudaSuccess;
+    if (ce == cudaSuccess) ce = up(h->d_fc, mv->fc_con, 8 * (size_t) h->Nf);
+    if (ce == cudaSuccess) ce = up(d_fn, mv->fn_con, 8 * (size_t) h->Nf);
+    if (ce == cudaSuccess) ce = up(h->d_slot, slot.data(), sizeof(int2) * slot.size());
+    if (ce == cudaSuccess) ce = up(d_cnoff, mv->cn_off, 4 * (size_t) (h->Nc + 1));
+    if (ce == cudaSuccess) ce = up(d_cncon, mv->cn_con, 4 * (size_t) ncn);
+    if (ce == cudaSuccess) ce = up(d_cfoff, cf_off.data(), 4 * cf_off.size());
+    if (ce == cudaSuccess) ce = up(d_cfcon, cf_con.data(), 4 * cf_con.size());
+    if (ce == cudaSuccess) ce = up(d_nodes, mv->nodes, 16 * (size_t) h->Nn);
+    if (ce == cudaSuccess) {
+        hcfd::geom_xc_kernel<<<nblk(h->Nc, 256), 256, 0, st>>>(h->Nc, d_cnoff, d_cncon, d_nodes, d_xc);
+        hcfd::geom_face_kernel<<<nblk(h->Nf, 256), 256, 0, st>>>(h->Nf, h->F_BC, d_fn, h->d_fc, d_nodes, d_xc, h->d_geo64);
+        hcfd::geom_iv_kernel<<<nblk(h->Nc, 256), 256, 0, st>>>(h->Nc, h->F_BC, d_cfoff, d_cfcon, h->d_fc, h->d_geo64, h->d_iv64);
+        if (f32) {
+            hcfd::convert_geo_kernel<float><<<nblk(h->Nf, 256), 256, 0, st>>>(h->Nf, h->d_geo64, (hcfd::FaceGeo<float>*) h->d_geo);
+            hcfd::convert_iv_kernel<float><<<nblk(h->Nc, 256), 256, 0, st>>>(h->Nc, h->d_iv64, (float*) h->d_iv);
+        } else {
+            ce = cudaMemcpyAsync(h->d_geo, h->d_geo64, sizeof(hcfd::FaceGeo<double>) * h->Nf, cudaMemcpyDeviceToDevice, st);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(h->d_iv, h->d_iv64, sizeof(double) * h->Nc, cudaMemcpyDeviceToDevice, st);
+        }
+        if (ce == cudaSuccess) ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) {
+        const unsigned long long inf2[2] = {0x7FF0000000000000ULL, 0x7FF0000000000000ULL};
+        ce = up(h->d_dtmin, inf2, sizeof(inf2));
+    }
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned int), st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_stats, 0, sizeof(hcfd::StepStats), st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_phiG, 0, tsz * 8 * h->Nc, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    free_tmp();
+    if (ce != cudaSuccess) return bail(fail(HCFD_ECUDA, std::string("gpu_create: ") + cudaGetErrorString(ce)));
+    *out = s.release();
+    return HCFD_OK;
+}
+
+int hcfd_gpu_gather_bcs(hcfd_solver* s, const int* bcmap, int nbcmap, const double* qbc) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!bcmap || !qbc || nbcmap <= 0) return fail(HCFD_EINVAL, "gather_bcs: bad argument");
+    // Euler::gather_BCs (src/Base/Euler.cpp:42-60).
+    hcfd::BCTable bc{};
+    bc.nbc = s->NBC;
+    const int fcolBC = s->Ncol - s->NBC;
+    for (int fcol = fcolBC; fcol < s->Ncol; fcol++) {
+        const int b = fcol - fcolBC;
+        const int tag = s->coltag[fcol];
+        if (tag < 0 || tag >= nbcmap) return fail(HCFD_EINVAL, "gather_bcs: colour tag outside the BC map");
+        const int t = bcmap[tag];
+        if (t < HCFD_SYMMETRY || t > HCFD_SUBOUTLET) return fail(HCFD_EINVAL, "gather_bcs: unknown BC type");
+        bc.type[b] = t;
+        bc.F1[b] = s->coloff[fcol];
+        for (int v = 0; v < 4; v++) bc.QBC[b][v] = qbc[4 * b + v];
+        prim_to_cons(bc.QBC[b], s->prm.gma, bc.UBC[b]);
+    }
+    bc.F1[s->NBC] = s->Nf;
+    s->bc = bc;
+    s->bcs_set = true;
+    return HCFD_OK;
+}
+
+int hcfd_gpu_initialise(hcfd_solver* s, const double* qic) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!qic) return fail(HCFD_EINVAL, "initialise: null state");
+    if (!s->bcs_set && s->NBC > 0) return fail(HCFD_EINVAL, "initialise: call gather_bcs first");
+    // Euler::initialise (src/Base/Euler.cpp:62-77).
+    double u[4];
+    prim_to_cons(qic, s->prm.gma, u);
+    s->cur = 0;
+    if (s->fp32()) hcfd::fill_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (hcfd::Cell4<float>*) s->d_U[0], u[0], u[1], u[2], u[3]);
+    else hcfd::fill_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (hcfd::Cell4<double>*) s->d_U[0], u[0], u[1], u[2], u[3]);
+    CK(cudaGetLastError());
+    rc = s->fp32() ? refresh_ghosts<float>(s) : refresh_ghosts<double>(s);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(s->d_stats, 0, sizeof(hcfd::StepStats), s->stream));
+    const unsigned long long inf2[2] = {0x7FF0000000000000ULL, 0x7FF0000000000000ULL};
+    CK(cudaMemcpyAsync(s->d_dtmin, inf2, sizeof(inf2), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->initialised = true;
+    return HCFD_OK;
+}
+
+int hcfd_gpu_step(hcfd_solver* s, int nsteps, int time_mode, double dt_or_cfl, hcfd_step_stats* stats) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!s->initialised) return fail(HCFD_EINVAL, "step: call initialise first");
+    if (nsteps < 0 || time_mode < HCFD_FIXED_DT || time_mode > HCFD_LOCAL_CFL || !std::isfinite(dt_or_cfl) || dt_or_cfl < 0)
+        return fail(HCFD_EINVAL, "step: bad argument");
+    for (int i = 0; i < nsteps; i++) {
+        rc = s->fp32() ? launch_step_w<float>(s, time_mode, dt_or_cfl) : launch_step_w<double>(s, time_mode, dt_or_cfl);
+        if (rc) return rc;
+    }
+    if (stats) return read_stats(s, stats);
+    return HCFD_OK;
+}
+
+int hcfd_gpu_stats(hcfd_solver* s, hcfd_step_stats* stats) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    return read_stats(s, stats);
+}
+
+int hcfd_gpu_sync(hcfd_solver* s) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+    return read_stats(s, nullptr);
+}
+
+int hcfd_gpu_download(hcfd_solver* s, int prims, double* const* out) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!out) return fail(HCFD_EINVAL, "download: null output");
+    for (int v = 0; v < 4; v++) if (!out[v]) return fail(HCFD_EINVAL, "download: null output array");
+    if (s->fp32()) hcfd::out_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<float>*) s->d_U[s->cur], s->prm.gma, prims, s->d_io);
+    else hcfd::out_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<double>*) s->d_U[s->cur], s->prm.gma, prims, s->d_io);
+    CK(cudaGetLastError());
+    for (int v = 0; v < 4; v++)
+        CK(cudaMemcpyAsync(out[v], s->d_io + (size_t) v * s->Nc, sizeof(double) * s->Nc, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return HCFD_OK;
+}
+
+int hcfd_gpu_upload(hcfd_solver* s, const double* const* in) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!in) return fail(HCFD_EINVAL, "upload: null input");
+    for (int v = 0; v < 4; v++) {
+        if (!in[v]) return fail(HCFD_EINVAL, "upload: null input array");
+        CK(cudaMemcpyAsync(s->d_io + (size_t) v * s->Nc, in[v], sizeof(double) * s->Nc, cudaMemcpyHostToDevice, s->stream));
+    }
+    if (s->fp32()) hcfd::in_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, s->d_io, (hcfd::Cell4<float>*) s->d_U[s->cur]);
+    else hcfd::in_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, s->d_io, (hcfd::Cell4<double>*) s->d_U[s->cur]);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
+    s->initialised = true;
+    return HCFD_OK;
+}
+
+int hcfd_gpu_wall_cp(hcfd_solver* s, int colour, double rho_inf, double p_inf, double speed_inf, double* out, int* n) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (colour < 0 || colour >= s->Ncol || !out || !n) return fail(HCFD_EINVAL, "wall_cp: bad argument");
+    const int F1 = s->coloff[colour], F2 = s->coloff[colour + 1];
+    const double qinf = 0.5 * rho_inf * speed_inf * speed_inf;
+    *n = F2 - F1;
+    if (F2 == F1) return HCFD_OK;
+    if (s->fp32()) hcfd::wall_cp_kernel<float><<<nblk(F2 - F1, 256), 256, 0, s->stream>>>(F1, F2, s->d_fc, (const hcfd::Cell4<float>*) s->d_U[s->cur], s->prm.gma, p_inf, qinf, s->d_cp);
+    else hcfd::wall_cp_kernel<double><<<nblk(F2 - F1, 256), 256, 0, s->stream>>>(F1, F2, s->d_fc, (const hcfd::Cell4<double>*) s->d_U[s->cur], s->prm.gma, p_inf, qinf, s->d_cp);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, s->d_cp, sizeof(double) * (F2 - F1), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return HCFD_OK;
+}
+
+int hcfd_gpu_info(hcfd_solver* s, int* Nc, int* Nf, int* Nreal, int* slots) {
+    if (!s) return fail(HCFD_EINVAL, "info: null handle");
+    if (Nc) *Nc = s->Nc;
+    if (Nf) *Nf = s->Nf;
+    if (Nreal) *Nreal = s->Nreal;
+    if (slots) *slots = s->W;
+    return HCFD_OK;
+}
+
+int hcfd_gpu_profile(hcfd_solver* s, int enable) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+    for (auto e : s->ev1) cudaEventDestroy(e);
+    for (auto e : s->ev2) cudaEventDestroy(e);
+    s->ev1.clear(); s->ev2.clear();
+    s->ms1 = s->ms2 = 0; s->n1 = s->n2 = 0;
+    s->prof = enable != 0;
+    return HCFD_OK;
+}
+
+int hcfd_gpu_profile_read(hcfd_solver* s, double* ms_pass1, long long* n_pass1, double* ms_pass2, long long* n_pass2) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+    for (size_t i = 0; i + 1 < s->ev1.size(); i += 2) {
+        float ms = 0; CK(cudaEventElapsedTime(&ms, s->ev1[i], s->ev1[i + 1])); s->ms1 += ms; s->n1++;
+        cudaEventDestroy(s->ev1[i]); cudaEventDestroy(s->ev1[i + 1]);
+    }
+    for (size_t i = 0; i + 1 < s->ev2.size(); i += 2) {
+        float ms = 0; CK(cudaEventElapsedTime(&ms, s->ev2[i], s->ev2[i + 1])); s->ms2 += ms; s->n2++;
+        cudaEventDestroy(s->ev2[i]); cudaEventDestroy(s->ev2[i + 1]);
+    }
+    s->ev1.clear(); s->ev2.clear();
+    if (ms_pass1) *ms_pass1 = s->ms1;
+    if (n_pass1) *n_pass1 = s->n1;
+    if (ms_pass2) *ms_pass2 = s->ms2;
+    if (n_pass2) *n_pass2 = s->n2;
+    return HCFD_OK;
+}
+
+void hcfd_gpu_destroy(hcfd_solver* s) {
+    if (!s) return;
+    free_all(s);
+    delete s;
+}
+
+}  // extern "C"

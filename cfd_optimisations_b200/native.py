@@ -1,0 +1,105 @@
+"""ctypes binding of libhcfd_gpu.so (include/hcfd_gpu.h).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libhcfd_gpu.so")
+
+# status codes (include/hcfd_gpu.h)
+OK, EINVAL, ENOMEM, ECUDA, ENONFINITE, ETIMEOUT, EIO, EAGAIN = 0, -1, -2, -3, -4, -5, -6, -7
+# includes/Base/BoundaryConditions.hpp:6-13
+SYMMETRY, WALL, SUPINLET, SUBINLET, SUPOUTLET, SUBOUTLET = range(6)
+LIMITER_BJ, LIMITER_VENKAT = 0, 1
+FIXED_DT, GLOBAL_CFL, LOCAL_CFL = 0, 1, 2
+FP64, FP32 = 0, 1
+NUMBER_NATURAL, NUMBER_RANDOM, NUMBER_RCM, NUMBER_MORTON = 0, 1, 2, 3
+
+_dp = ct.POINTER(ct.c_double)
+_ip = ct.POINTER(ct.c_int)
+
+
+class MeshView(ct.Structure):
+    _fields_ = [("dim", ct.c_int), ("Nn", ct.c_int), ("Ncol", ct.c_int), ("NBCcol", ct.c_int),
+                ("Nc", ct.c_int), ("Nf", ct.c_int),
+                ("coltag", _ip), ("coloff", _ip), ("nodes", _dp), ("fn_con", _ip), ("fc_con", _ip),
+                ("cn_off", _ip), ("cn_con", _ip), ("cc_off", _ip), ("cc_con", _ip)]
+
+
+class WedgeSpec(ct.Structure):
+    _fields_ = [("nx", ct.c_int), ("ny", ct.c_int), ("length", ct.c_double), ("height", ct.c_double),
+                ("x_ramp", ct.c_double), ("theta_deg", ct.c_double), ("jitter", ct.c_double),
+                ("seed", ct.c_uint64), ("numbering", ct.c_int)]
+
+
+class Params(ct.Structure):
+    _fields_ = [("gma", ct.c_double), ("limiter", ct.c_int), ("venkat_K", ct.c_double),
+                ("precision", ct.c_int), ("block", ct.c_int)]
+
+
+class StepStats(ct.Structure):
+    _fields_ = [("dt", ct.c_double), ("res_l2", ct.c_double), ("res_first", ct.c_double),
+                ("steps", ct.c_longlong), ("nonfinite", ct.c_int)]
+
+
+class HcfdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"hcfd error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "hcfd_mesh_load": (ct.c_int, [ct.c_char_p, ct.POINTER(ct.c_void_p)]),
+    "hcfd_mesh_write": (ct.c_int, [ct.c_void_p, ct.c_char_p]),
+    "hcfd_mesh_view_of": (ct.c_int, [ct.c_void_p, ct.POINTER(MeshView)]),
+    "hcfd_mesh_cf": (ct.c_int, [ct.c_void_p, ct.POINTER(_ip), ct.POINTER(_ip)]),
+    "hcfd_mesh_pname": (ct.c_char_p, [ct.c_void_p, ct.c_int]),
+    "hcfd_mesh_free": (None, [ct.c_void_p]),
+    "hcfd_mesh_generate_wedge": (ct.c_int, [ct.POINTER(WedgeSpec), ct.POINTER(ct.c_void_p)]),
+    "hcfd_mesh_renumber": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_uint64]),
+    "hcfd_gpu_create": (ct.c_int, [ct.POINTER(MeshView), ct.POINTER(Params), ct.POINTER(ct.c_void_p)]),
+    "hcfd_gpu_gather_bcs": (ct.c_int, [ct.c_void_p, _ip, ct.c_int, _dp]),
+    "hcfd_gpu_initialise": (ct.c_int, [ct.c_void_p, _dp]),
+    "hcfd_gpu_step": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double, ct.POINTER(StepStats)]),
+    "hcfd_gpu_download": (ct.c_int, [ct.c_void_p, ct.c_int, ct.POINTER(_dp)]),
+    "hcfd_gpu_upload": (ct.c_int, [ct.c_void_p, ct.POINTER(_dp)]),
+    "hcfd_gpu_sync": (ct.c_int, [ct.c_void_p]),
+    "hcfd_gpu_stats": (ct.c_int, [ct.c_void_p, ct.POINTER(StepStats)]),
+    "hcfd_gpu_wall_cp": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double, ct.c_double, ct.c_double, _dp, _ip]),
+    "hcfd_gpu_info": (ct.c_int, [ct.c_void_p, _ip, _ip, _ip, _ip]),
+    "hcfd_gpu_profile": (ct.c_int, [ct.c_void_p, ct.c_int]),
+    "hcfd_gpu_profile_read": (ct.c_int, [ct.c_void_p, _dp, ct.POINTER(ct.c_longlong), _dp, ct.POINTER(ct.c_longlong)]),
+    "hcfd_gpu_destroy": (None, [ct.c_void_p]),
+    "hcfd_write_hsln": (ct.c_int, [ct.c_char_p, ct.c_int, ct.POINTER(ct.c_char_p), ct.c_int, ct.POINTER(_dp)]),
+    "hcfd_last_error": (ct.c_char_p, []),
+}
+
+
+def lib():
+    """The loaded native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"native library missing: {LIB_PATH}; build it with "
+                               f"`python -m cfd_optimisations_b200._build` (there is no CPU fallback)")
+        L = ct.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> int:
+    if rc != OK:
+        msg = lib().hcfd_last_error()
+        raise HcfdError(rc, msg.decode() if msg else "")
+    return rc

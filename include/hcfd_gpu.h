@@ -1,0 +1,203 @@
+/* hcfd_gpu.h — C ABI of the B200 solver for the per-step residual-and-update loop of the
+ * 2-D unstructured cell-centred finite-volume Euler solver of
+ * Hasti-Jalal-Aldeen/CFD_Optimisations.
+ *
+ * Every entry point below names the reference interface it stands in for.  The reference
+ * has no C ABI of its own: its solver is a set of C++ classes (includes/Base/*.hpp) built
+ * into one executable, and its only historical foreign-function boundary was a ctypes
+ * binding (interface/LEGACY/Run.py:98-141).  This header is what such a binding, or the
+ * C++ drop-in in hcfd_gpu.hpp, calls.
+ *
+ * Conventions
+ *  - Plain pointers and sizes, no C++ types.  Status codes: HCFD_OK (0) or a negative
+ *    HCFD_E* value; hcfd_last_error() gives the text of the last failure on the calling
+ *    thread.
+ *  - Host arrays passed in are copied; the caller keeps ownership.  The library owns all
+ *    device memory.  Each solver handle owns one CUDA stream; a handle is not thread-safe,
+ *    distinct handles may be used from distinct threads.
+ *  - State arrays are variable-major (4 arrays of Nc doubles: rho, rho u, rho v, E), the
+ *    layout of the reference's `double* U[NVARS]` (includes/Base/TimeIntegrators.hpp:38-42).
+ *  - There is no CPU fallback: without a usable CUDA device every solver call fails with
+ *    HCFD_ECUDA.
+ */
+#ifndef HCFD_GPU_H
+#define HCFD_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------- */
+#define HCFD_OK           0
+#define HCFD_EINVAL      -1   /* bad argument or malformed mesh                            */
+#define HCFD_ENOMEM      -2   /* host or device allocation failed                          */
+#define HCFD_ECUDA       -3   /* CUDA runtime error (no device, launch failure, ...)       */
+#define HCFD_ENONFINITE  -4   /* a NaN or Inf appeared in the state                        */
+#define HCFD_ETIMEOUT    -5   /* a bounded device wait gave up                             */
+#define HCFD_EIO         -6   /* file could not be read or written                         */
+#define HCFD_EAGAIN      -7   /* arena full: retry after a retirement                      */
+
+/* Boundary-condition types, same values as Base::BCtype
+ * (includes/Base/BoundaryConditions.hpp:6-13). */
+enum hcfd_bctype {
+    HCFD_SYMMETRY = 0, HCFD_WALL = 1, HCFD_SUPINLET = 2,
+    HCFD_SUBINLET = 3, HCFD_SUPOUTLET = 4, HCFD_SUBOUTLET = 5
+};
+
+/* Limiter: Barth-Jespersen (the reference's Limiter::limit_gradient,
+ * src/Base/Limiter.cpp:19-77) or Venkatakrishnan with constant K (not in the reference). */
+enum hcfd_limiter { HCFD_LIMITER_BJ = 0, HCFD_LIMITER_VENKAT = 1 };
+
+/* How a step picks dt.  HCFD_FIXED_DT is the reference's only mode (Euler::run(T, dt,
+ * dt_out), src/Base/Euler.cpp:79-105).  The CFL modes are not in the reference. */
+enum hcfd_time_mode { HCFD_FIXED_DT = 0, HCFD_GLOBAL_CFL = 1, HCFD_LOCAL_CFL = 2 };
+
+/* Arithmetic of the step.  HCFD_FP64 follows the reference's double arithmetic.
+ * HCFD_FP32 keeps state, gradients, limiter and fluxes in float, sums each cell's face
+ * fluxes with a compensated (two-sum) accumulator, and keeps geometry precompute and the
+ * residual-norm reduction in double. */
+enum hcfd_precision { HCFD_FP64 = 0, HCFD_FP32 = 1 };
+
+/* Cell renumbering applied by hcfd_mesh_renumber. */
+enum hcfd_numbering {
+    HCFD_NUMBER_NATURAL = 0, HCFD_NUMBER_RANDOM = 1, HCFD_NUMBER_RCM = 2, HCFD_NUMBER_MORTON = 3
+};
+
+/* ---- meshes ------------------------------------------------------------------------- */
+
+/* The public raw arrays of the reference's Mesh (includes/Mesh.hpp:4-22).  Cells include
+ * the boundary ghost cells (the mesh's line elements); faces are grouped by colour in
+ * coloff order, interior colour(s) first, then NBCcol boundary colours, and every boundary
+ * face has its ghost cell on the right (fc_con[2f+1]).  cc_off/cc_con may be NULL. */
+typedef struct hcfd_mesh_view {
+    int dim, Nn, Ncol, NBCcol, Nc, Nf;
+    const int*    coltag;   /* [Ncol]            */
+    const int*    coloff;   /* [Ncol+1]          */
+    const double* nodes;    /* [Nn*dim]          */
+    const int*    fn_con;   /* [2*Nf]            */
+    const int*    fc_con;   /* [2*Nf]            */
+    const int*    cn_off;   /* [Nc+1]            */
+    const int*    cn_con;   /* [cn_off[Nc]]      */
+    const int*    cc_off;   /* [Nc+1] or NULL    */
+    const int*    cc_con;   /* [cc_off[Nc]]      */
+} hcfd_mesh_view;
+
+typedef struct hcfd_mesh hcfd_mesh;   /* host mesh owned by the library */
+
+/* Replaces Mesh::Mesh(const char* fname) (src/Mesh.cpp:7-54).  Unlike the reference it
+ * checks the file: a missing, truncated or inconsistent .hmsh gives HCFD_EIO/HCFD_EINVAL. */
+int  hcfd_mesh_load(const char* path, hcfd_mesh** out);
+/* Writes the .hmsh layout of interface/Mesh.py:441-463 (header, names, coltag, coloff,
+ * nodes, fn_con, fc_con, cn_off, cn_con, cc_off, cc_con, c_ctypes). */
+int  hcfd_mesh_write(const hcfd_mesh* m, const char* path);
+/* Fills *v with pointers into m (valid until m is freed or renumbered). */
+int  hcfd_mesh_view_of(const hcfd_mesh* m, hcfd_mesh_view* v);
+/* The CSR cell->face table of Mesh::compute_cf_con (src/Mesh.cpp:88-117): the faces of
+ * cell c, in increasing face index, are cf_con[cf_off[c] .. cf_off[c+1]). */
+int  hcfd_mesh_cf(const hcfd_mesh* m, const int** cf_off, const int** cf_con);
+/* Physical name k (the reference's Mesh::pnames, src/Mesh.cpp:70-86) or NULL. */
+const char* hcfd_mesh_pname(const hcfd_mesh* m, int k);
+void hcfd_mesh_free(hcfd_mesh* m);
+
+/* Supersonic-wedge generator (the mesh family of the reference's wedge.hmsh, produced
+ * here directly instead of through gmsh and interface/Mesh.py).  Domain x in [0, length],
+ * top wall y = height, bottom wall y_b(x) = max(0, (x - x_ramp) tan(theta)).  nx x ny
+ * nodes mapped vertically between y_b and the top; interior nodes jittered by
+ * U(-jitter, jitter) times the local spacing in x and y; each quad split into two
+ * triangles along a diagonal picked by a seeded coin flip; one ghost line cell per
+ * boundary edge.  Colours: 0 interior, 1 "upper", 2 "lower", 3 "inlet", 4 "outlet"
+ * (the colour tags of the reference's wedge.hmsh, driven by src/Test.cpp:64).  Cells are
+ * then renumbered by `numbering` (the random permutation uses `seed` too). */
+typedef struct hcfd_wedge_spec {
+    int      nx, ny;
+    double   length, height, x_ramp, theta_deg, jitter;
+    uint64_t seed;
+    int      numbering;   /* enum hcfd_numbering */
+} hcfd_wedge_spec;
+int  hcfd_mesh_generate_wedge(const hcfd_wedge_spec* spec, hcfd_mesh** out);
+/* Renumbers the cells (ghosts included) and re-sorts faces inside each colour by
+ * (min cell, max cell), with interior faces oriented CL < CR and boundary faces keeping
+ * the ghost on the right: the face order interface/Mesh.py:321-378 produces. */
+int  hcfd_mesh_renumber(hcfd_mesh* m, int numbering, uint64_t seed);
+
+/* ---- solver ------------------------------------------------------------------------- */
+
+typedef struct hcfd_params {
+    double gma;         /* ratio of specific heats, Flux(nvars, gma, domain) (includes/Base/Flux.hpp:9) */
+    int    limiter;     /* enum hcfd_limiter                                                 */
+    double venkat_K;    /* Venkatakrishnan constant (limiter == HCFD_LIMITER_VENKAT)         */
+    int    precision;   /* enum hcfd_precision                                               */
+    int    block;       /* threads per block of the step kernels, 0 = default               */
+} hcfd_params;
+
+typedef struct hcfd_step_stats {
+    double dt;          /* dt of the last step (minimum local dt under HCFD_LOCAL_CFL)       */
+    double res_l2;      /* L2 density residual of the last step, sqrt(sum R_rho^2 / Nreal)   */
+    double res_first;   /* residual of the first step this handle took                       */
+    long long steps;    /* steps taken by this handle since hcfd_gpu_initialise              */
+    int    nonfinite;   /* 1 if the last step produced a NaN or Inf residual                 */
+} hcfd_step_stats;
+
+typedef struct hcfd_solver hcfd_solver;
+
+/* Replaces Domain(Mesh&) + GaussGreen(const Domain&) + Limiter(const Domain&) +
+ * Flux(nvars, gma, const Domain&) + Euler(nvars, Domain&, ...) (includes/Base/Domain.hpp:26,
+ * GradientSchemes.hpp:8, Limiters.hpp:8, Flux.hpp:9, TimeIntegrators.hpp:13): uploads the
+ * mesh, computes the geometry on the device in double (src/Base/Domain.cpp:4-154, with
+ * zero_bc_iv as the Euler constructor applies it, src/Base/Euler.cpp:24) and allocates
+ * the state. */
+int  hcfd_gpu_create(const hcfd_mesh_view* mesh, const hcfd_params* params, hcfd_solver** out);
+/* Replaces Euler::gather_BCs(const BCtype* BCmap, const double QBC[][NVARS])
+ * (src/Base/Euler.cpp:42-60): boundary colour k takes type bcmap[coltag[colour]] and the
+ * primitive state qbc[4*k .. 4*k+3]. */
+int  hcfd_gpu_gather_bcs(hcfd_solver* s, const int* bcmap, int nbcmap, const double* qbc);
+/* Replaces Euler::initialise(const double QIC[NVARS]) (src/Base/Euler.cpp:62-77). */
+int  hcfd_gpu_initialise(hcfd_solver* s, const double* qic);
+/* Runs nsteps iterations of the body of Euler::run's loop (src/Base/Euler.cpp:86-96):
+ * gradient, limiter, ghost gradients/limiter, flux, U += dt R, ghost cells.  dt_or_cfl is
+ * dt under HCFD_FIXED_DT and the CFL number otherwise.  Enqueued on the handle's stream;
+ * when stats is non-NULL the call waits and fills it. */
+int  hcfd_gpu_step(hcfd_solver* s, int nsteps, int time_mode, double dt_or_cfl, hcfd_step_stats* stats);
+/* Euler::compute_prims + copy-out (src/Base/Euler.cpp:115-136): prims != 0 gives
+ * (rho, u, v, p), else the conservative state.  out[v] holds Nc doubles. */
+int  hcfd_gpu_download(hcfd_solver* s, int prims, double* const* out);
+/* Overwrites the conservative state from 4 host arrays of Nc doubles (checkpoint
+ * restore; no reference counterpart). */
+int  hcfd_gpu_upload(hcfd_solver* s, const double* const* in);
+/* Waits for the handle's stream; returns HCFD_ENONFINITE if a step produced a NaN/Inf. */
+int  hcfd_gpu_sync(hcfd_solver* s);
+/* Statistics of the steps taken so far (waits for the stream). */
+int  hcfd_gpu_stats(hcfd_solver* s, hcfd_step_stats* stats);
+/* Wall pressure coefficient (p_CL - p_inf) / (0.5 rho_inf |u_inf|^2) on the faces of one
+ * colour, in face order; *n gets the face count.  No reference counterpart. */
+int  hcfd_gpu_wall_cp(hcfd_solver* s, int colour, double rho_inf, double p_inf, double speed_inf,
+                      double* out, int* n);
+/* Mesh facts as the solver sees them: Nc, Nf, number of real (non-ghost) cells, the
+ * face slots per cell of the step kernels. */
+int  hcfd_gpu_info(hcfd_solver* s, int* Nc, int* Nf, int* Nreal, int* slots);
+/* Per-kernel timing with CUDA events on the handle's stream.  enable != 0 starts
+ * recording every launch of the two step kernels; hcfd_gpu_profile_read returns the
+ * summed milliseconds and launch counts since enabling. */
+int  hcfd_gpu_profile(hcfd_solver* s, int enable);
+int  hcfd_gpu_profile_read(hcfd_solver* s, double* ms_pass1, long long* n_pass1,
+                           double* ms_pass2, long long* n_pass2);
+void hcfd_gpu_destroy(hcfd_solver* s);
+
+/* ---- output ------------------------------------------------------------------------- */
+
+/* Replaces Writer::write_soln (src/Writer.cpp:22-39): writes int32 Nc, nvars, nchars,
+ * the NUL-terminated names, then nvars x Nc doubles to `path` (the caller forms the
+ * reference's "<fname>_<runcount>.hsln" name). */
+int  hcfd_write_hsln(const char* path, int nvars, const char* const* varnames, int Nc,
+                     const double* const* arrs);
+
+/* ---- errors ------------------------------------------------------------------------- */
+const char* hcfd_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HCFD_GPU_H */

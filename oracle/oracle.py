@@ -28,6 +28,8 @@ REF_SO = os.path.join(HERE, "_ref", "libhcfd_ref.so")
 SYMMETRY, WALL, SUPINLET, SUBINLET, SUPOUTLET, SUBOUTLET = range(6)
 BJ, VENKAT = 0, 1
 FIXED_DT, GLOBAL_CFL, LOCAL_CFL = 0, 1, 2
+# fields of Oracle.get (hcfd_oracle.h)
+F_U, F_Q, F_PHI, F_R, F_G, F_DTLOC, F_IV = range(7)
 
 _dp = ct.POINTER(ct.c_double)
 _ip = ct.POINTER(ct.c_int)
