@@ -163,6 +163,15 @@ class Solver:
         return dict(dt=st.dt, res_l2=st.res_l2, res_first=st.res_first, steps=st.steps,
                     nonfinite=bool(st.nonfinite))
 
+    def step_timed(self, nsteps: int, mode: int = FIXED_DT, dt_or_cfl: float = 1e-3) -> float:
+        """Runs nsteps steps; returns their device time in ms (CUDA events on the handle's stream)."""
+        ms = ct.c_double()
+        _n.check(_n.lib().hcfd_gpu_step_timed(self._h, nsteps, mode, dt_or_cfl, ct.byref(ms)))
+        return ms.value
+
+    def launches_per_step(self) -> int:
+        return _n.lib().hcfd_gpu_launches_per_step(self._h)
+
     def stats(self) -> dict:
         st = _n.StepStats()
         _n.check(_n.lib().hcfd_gpu_stats(self._h, ct.byref(st)))
@@ -202,6 +211,26 @@ class Solver:
         n1, n2 = ct.c_longlong(), ct.c_longlong()
         _n.check(_n.lib().hcfd_gpu_profile_read(self._h, ct.byref(m1), ct.byref(n1), ct.byref(m2), ct.byref(n2)))
         return dict(ms_pass1=m1.value, n_pass1=n1.value, ms_pass2=m2.value, n_pass2=n2.value)
+
+
+def set_device(device: int) -> int:
+    """Selects the CUDA device for handles created afterwards; returns the device count."""
+    n = ct.c_int()
+    _n.check(_n.lib().hcfd_set_device(device, ct.byref(n)))
+    return n.value
+
+
+def device_sync() -> None:
+    _n.check(_n.lib().hcfd_device_sync())
+
+
+def pin(a: np.ndarray) -> None:
+    """Page-locks a numpy array's memory for direct DMA (cudaHostRegister)."""
+    _n.check(_n.lib().hcfd_host_pin(ct.c_void_p(a.ctypes.data), a.nbytes))
+
+
+def unpin(a: np.ndarray) -> None:
+    _n.check(_n.lib().hcfd_host_unpin(ct.c_void_p(a.ctypes.data)))
 
 
 def write_hsln(path: str, arrs, varnames=("Density", "Velocity_X", "Velocity_Y", "Pressure")) -> None:

@@ -471,6 +471,59 @@ int hcfd_gpu_profile_read(hcfd_solver* s, double* ms_pass1, long long* n_pass1, 
     return HCFD_OK;
 }
 
+int hcfd_gpu_step_timed(hcfd_solver* s, int nsteps, int time_mode, double dt_or_cfl, double* ms) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!ms) return fail(HCFD_EINVAL, "step_timed: null output");
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, s->stream));
+    rc = hcfd_gpu_step(s, nsteps, time_mode, dt_or_cfl, nullptr);
+    if (rc) { cudaEventDestroy(a); cudaEventDestroy(b); return rc; }
+    CK(cudaEventRecord(b, s->stream));
+    CK(cudaEventSynchronize(b));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = t;
+    return read_stats(s, nullptr);
+}
+
+int hcfd_gpu_launches_per_step(hcfd_solver* s) { return s ? 2 : 0; }
+
+int hcfd_host_pin(void* p, size_t bytes) {
+    hcfd::clear_error();
+    if (!p || !bytes) return fail(HCFD_EINVAL, "host_pin: bad argument");
+    CK(cudaHostRegister(p, bytes, cudaHostRegisterDefault));
+    return HCFD_OK;
+}
+
+int hcfd_host_unpin(void* p) {
+    hcfd::clear_error();
+    if (!p) return fail(HCFD_EINVAL, "host_unpin: null pointer");
+    CK(cudaHostUnregister(p));
+    return HCFD_OK;
+}
+
+int hcfd_set_device(int device, int* count) {
+    hcfd::clear_error();
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    if (count) *count = n;
+    if (device < 0 || device >= n) return fail(HCFD_EINVAL, "set_device: no such device");
+    CK(cudaSetDevice(device));
+    return HCFD_OK;
+}
+
+int hcfd_device_sync(void) {
+    hcfd::clear_error();
+    CK(cudaDeviceSynchronize());
+    return HCFD_OK;
+}
+
 void hcfd_gpu_destroy(hcfd_solver* s) {
     if (!s) return;
     free_all(s);

@@ -76,8 +76,14 @@ _SIGS = {
     "hcfd_gpu_info": (ct.c_int, [ct.c_void_p, _ip, _ip, _ip, _ip]),
     "hcfd_gpu_profile": (ct.c_int, [ct.c_void_p, ct.c_int]),
     "hcfd_gpu_profile_read": (ct.c_int, [ct.c_void_p, _dp, ct.POINTER(ct.c_longlong), _dp, ct.POINTER(ct.c_longlong)]),
+    "hcfd_gpu_step_timed": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double, _dp]),
+    "hcfd_gpu_launches_per_step": (ct.c_int, [ct.c_void_p]),
     "hcfd_gpu_destroy": (None, [ct.c_void_p]),
+    "hcfd_host_pin": (ct.c_int, [ct.c_void_p, ct.c_size_t]),
+    "hcfd_host_unpin": (ct.c_int, [ct.c_void_p]),
     "hcfd_write_hsln": (ct.c_int, [ct.c_char_p, ct.c_int, ct.POINTER(ct.c_char_p), ct.c_int, ct.POINTER(_dp)]),
+    "hcfd_set_device": (ct.c_int, [ct.c_int, _ip]),
+    "hcfd_device_sync": (ct.c_int, []),
     "hcfd_last_error": (ct.c_char_p, []),
 }
 

@@ -184,7 +184,18 @@ int  hcfd_gpu_info(hcfd_solver* s, int* Nc, int* Nf, int* Nreal, int* slots);
 int  hcfd_gpu_profile(hcfd_solver* s, int enable);
 int  hcfd_gpu_profile_read(hcfd_solver* s, double* ms_pass1, long long* n_pass1,
                            double* ms_pass2, long long* n_pass2);
+/* Runs nsteps steps as hcfd_gpu_step does and waits; *ms gets the device time between two
+ * CUDA events recorded on the handle's stream before the first and after the last launch.
+ * No reference counterpart (the reference times whole runs with clock(), src/Test.cpp:72-74). */
+int  hcfd_gpu_step_timed(hcfd_solver* s, int nsteps, int time_mode, double dt_or_cfl, double* ms);
+/* Number of kernel launches one step issues (the two passes). */
+int  hcfd_gpu_launches_per_step(hcfd_solver* s);
 void hcfd_gpu_destroy(hcfd_solver* s);
+
+/* Page-locks a caller-owned host range (cudaHostRegister) so that hcfd_gpu_upload and
+ * hcfd_gpu_download from and to it run as direct DMA; hcfd_host_unpin releases it. */
+int  hcfd_host_pin(void* p, size_t bytes);
+int  hcfd_host_unpin(void* p);
 
 /* ---- output ------------------------------------------------------------------------- */
 
@@ -193,6 +204,15 @@ void hcfd_gpu_destroy(hcfd_solver* s);
  * reference's "<fname>_<runcount>.hsln" name). */
 int  hcfd_write_hsln(const char* path, int nvars, const char* const* varnames, int Nc,
                      const double* const* arrs);
+
+/* ---- devices ------------------------------------------------------------------------ */
+
+/* Makes `device` the calling thread's current CUDA device for the handles it creates
+ * afterwards (one process per GPU; a handle stays on the device it was created on).
+ * *count, if non-NULL, gets the number of visible devices. */
+int  hcfd_set_device(int device, int* count);
+/* Waits for all work on the current device (cudaDeviceSynchronize). */
+int  hcfd_device_sync(void);
 
 /* ---- errors ------------------------------------------------------------------------- */
 const char* hcfd_last_error(void);
