@@ -22,7 +22,7 @@ import ctypes as ct
 import numpy as np
 
 from . import native as _n
-from .native import (FIXED_DT, GLOBAL_CFL, LOCAL_CFL, FP32, FP64, LIMITER_BJ, LIMITER_VENKAT,
+from .native import (FIXED_DT, GLOBAL_CFL, LOCAL_CFL, FP32, FP64, KERNEL_CELL, KERNEL_TILED, LIMITER_BJ, LIMITER_VENKAT,
                      NUMBER_MORTON, NUMBER_NATURAL, NUMBER_RANDOM, NUMBER_RCM, SUBINLET, SUBOUTLET,
                      SUPINLET, SUPOUTLET, SYMMETRY, WALL, HcfdError)
 
@@ -124,10 +124,11 @@ class Solver:
     """One mesh on one GPU (include/hcfd_gpu.h, hcfd_gpu_*)."""
 
     def __init__(self, mesh: Mesh, gma: float = 1.4, limiter: int = LIMITER_BJ, venkat_K: float = 5.0,
-                 precision: int = FP64, block: int = 0):
+                 precision: int = FP64, block: int = 0, kernel: int = 0, tile: int = 0,
+                 keep_numbering: bool = False):
         self._mesh = mesh
         v = mesh.view()
-        p = _n.Params(gma, limiter, venkat_K, precision, block)
+        p = _n.Params(gma, limiter, venkat_K, precision, block, kernel, tile, 1 if keep_numbering else 0)
         h = ct.c_void_p()
         _n.check(_n.lib().hcfd_gpu_create(ct.byref(v), ct.byref(p), ct.byref(h)))
         self._h = h
@@ -211,6 +212,15 @@ class Solver:
         n1, n2 = ct.c_longlong(), ct.c_longlong()
         _n.check(_n.lib().hcfd_gpu_profile_read(self._h, ct.byref(m1), ct.byref(n1), ct.byref(m2), ct.byref(n2)))
         return dict(ms_pass1=m1.value, n_pass1=n1.value, ms_pass2=m2.value, n_pass2=n2.value)
+
+
+def plan_check(mesh: Mesh, tile: int = 0, keep_numbering: bool = False) -> dict:
+    """Builds and checks the tiled kernels' plan on the host (see hcfd_plan_check)."""
+    v = mesh.view()
+    info = (ct.c_longlong * 8)()
+    _n.check(_n.lib().hcfd_plan_check(ct.byref(v), tile, 1 if keep_numbering else 0, info))
+    keys = ("tiles", "halo_max", "entries_max", "entries", "faces_once", "faces_cut", "slots", "halo_total")
+    return dict(zip(keys, list(info)))
 
 
 def set_device(device: int) -> int:

@@ -32,4 +32,17 @@ int validate_view(const hcfd_mesh_view& v);
 // Builds cf_off/cf_con exactly as Mesh::compute_cf_con does (faces of each cell in
 // increasing face index).
 void build_cf(int Nc, int Nf, const int* fc_con, std::vector<int>& cf_off, std::vector<int>& cf_con);
+
+// Execution plan of the tiled step kernels (hcfd_plan.cpp).
+struct TilePlan {
+    int B = 256, W = 3, Wp = 4, ntiles = 0, Hmax = 0, Fmax = 0;
+    std::vector<int> foff, hoff, halo, efid;
+    std::vector<short> meta, cslot;
+};
+// Internal cell order: cells sorted by the Morton key of their vertex-average centre.
+// Returns perm with perm[internal] = input index.
+std::vector<int> morton_order(const hcfd_mesh_view& v);
+int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, const std::vector<int>& cf_con,
+                    const std::vector<char>& ghost, const std::vector<int>& perm, int F_BC,
+                    const std::vector<int>& bc_first, int B, int W, TilePlan& P);
 }  // namespace hcfd

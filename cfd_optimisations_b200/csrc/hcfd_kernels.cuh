@@ -85,22 +85,28 @@ struct StepArgs {
 // ---------------------------------------------------------------------------------------
 // loads
 
-__device__ __forceinline__ void ld_cell(const Cell4<double>* p, int i, double u[4]) {
-    const double2* q = reinterpret_cast<const double2*>(p + i);
-    double2 a = __ldg(q), b = __ldg(q + 1);
+// Per-cell records (the state Cell4 and the limited gradient Grad8) are stored as 16-byte
+// chunk planes: chunk j of record i sits at byte (j * ps + i) * 16 from the base, ps being the
+// plane stride in chunks (Nc in HBM, the staged cell count in shared memory).  Random
+// 16-byte gathers then spread over all shared-memory bank groups, and a warp's accesses to
+// consecutive records are contiguous in every plane.  Cell4: 2 chunks in double, 1 in
+// float; Grad8: 4 and 2.
+__device__ __forceinline__ void ld_cell(const Cell4<double>* p, size_t ps, int i, double u[4]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = __ldg(q + i), b = __ldg(q + ps + i);
     u[0] = a.x; u[1] = a.y; u[2] = b.x; u[3] = b.y;
 }
-__device__ __forceinline__ void ld_cell(const Cell4<float>* p, int i, float u[4]) {
-    float4 a = __ldg(reinterpret_cast<const float4*>(p + i));
+__device__ __forceinline__ void ld_cell(const Cell4<float>* p, size_t, int i, float u[4]) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p) + i);
     u[0] = a.x; u[1] = a.y; u[2] = a.z; u[3] = a.w;
 }
-__device__ __forceinline__ void st_cell(Cell4<double>* p, int i, const double u[4]) {
-    double2* q = reinterpret_cast<double2*>(p + i);
-    q[0] = make_double2(u[0], u[1]);
-    q[1] = make_double2(u[2], u[3]);
+__device__ __forceinline__ void st_cell(Cell4<double>* p, size_t ps, int i, const double u[4]) {
+    double2* q = reinterpret_cast<double2*>(p);
+    q[i] = make_double2(u[0], u[1]);
+    q[ps + i] = make_double2(u[2], u[3]);
 }
-__device__ __forceinline__ void st_cell(Cell4<float>* p, int i, const float u[4]) {
-    *reinterpret_cast<float4*>(p + i) = make_float4(u[0], u[1], u[2], u[3]);
+__device__ __forceinline__ void st_cell(Cell4<float>* p, size_t, int i, const float u[4]) {
+    reinterpret_cast<float4*>(p)[i] = make_float4(u[0], u[1], u[2], u[3]);
 }
 __device__ __forceinline__ void ld_geo(const FaceGeo<double>* p, int f, FaceGeo<double>& g) {
     const double2* q = reinterpret_cast<const double2*>(p + f);
@@ -112,27 +118,25 @@ __device__ __forceinline__ void ld_geo(const FaceGeo<float>* p, int f, FaceGeo<f
     float4 a = __ldg(q), b = __ldg(q + 1);
     g.nx = a.x; g.ny = a.y; g.Af = a.z; g.If = a.w; g.rLx = b.x; g.rLy = b.y; g.rRx = b.z; g.rRy = b.w;
 }
-// phiG of pass 1 is written and read within one step, so it is read through L2 (ld.cg
-// semantics are not needed: pass 2 is a separate launch).
-__device__ __forceinline__ void ld_grad(const Grad8<double>* p, int i, double g[8]) {
-    const double2* q = reinterpret_cast<const double2*>(p + i);
+__device__ __forceinline__ void ld_grad(const Grad8<double>* p, size_t ps, int i, double g[8]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
 #pragma unroll
-    for (int k = 0; k < 4; k++) { double2 a = __ldg(q + k); g[2 * k] = a.x; g[2 * k + 1] = a.y; }
+    for (int k = 0; k < 4; k++) { const double2 a = __ldg(q + k * ps + i); g[2 * k] = a.x; g[2 * k + 1] = a.y; }
 }
-__device__ __forceinline__ void ld_grad(const Grad8<float>* p, int i, float g[8]) {
-    const float4* q = reinterpret_cast<const float4*>(p + i);
-    float4 a = __ldg(q), b = __ldg(q + 1);
+__device__ __forceinline__ void ld_grad(const Grad8<float>* p, size_t ps, int i, float g[8]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 a = __ldg(q + i), b = __ldg(q + ps + i);
     g[0] = a.x; g[1] = a.y; g[2] = a.z; g[3] = a.w; g[4] = b.x; g[5] = b.y; g[6] = b.z; g[7] = b.w;
 }
-__device__ __forceinline__ void st_grad(Grad8<double>* p, int i, const double g[8]) {
-    double2* q = reinterpret_cast<double2*>(p + i);
+__device__ __forceinline__ void st_grad(Grad8<double>* p, size_t ps, int i, const double g[8]) {
+    double2* q = reinterpret_cast<double2*>(p);
 #pragma unroll
-    for (int k = 0; k < 4; k++) q[k] = make_double2(g[2 * k], g[2 * k + 1]);
+    for (int k = 0; k < 4; k++) q[k * ps + i] = make_double2(g[2 * k], g[2 * k + 1]);
 }
-__device__ __forceinline__ void st_grad(Grad8<float>* p, int i, const float g[8]) {
-    float4* q = reinterpret_cast<float4*>(p + i);
-    q[0] = make_float4(g[0], g[1], g[2], g[3]);
-    q[1] = make_float4(g[4], g[5], g[6], g[7]);
+__device__ __forceinline__ void st_grad(Grad8<float>* p, size_t ps, int i, const float g[8]) {
+    float4* q = reinterpret_cast<float4*>(p);
+    q[i] = make_float4(g[0], g[1], g[2], g[3]);
+    q[ps + i] = make_float4(g[4], g[5], g[6], g[7]);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -279,7 +283,7 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
         for (int k = 0; k < W; k++) s[k] = __ldg(a.slot + (size_t) k * a.Nc + c);
         if (s[0].y >= 0) {
             T u[4];
-            ld_cell(a.U, c, u);
+            ld_cell(a.U, a.Nc, c, u);
             const T iv = __ldg(a.iv + c);
             T G[4][2], umin[4], umax[4], ro[W][2];
 #pragma unroll
@@ -295,7 +299,7 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
                 FaceGeo<T> g;
                 ld_geo(a.geo, f, g);
                 T un[4];
-                ld_cell(a.U, s[k].y, un);
+                ld_cell(a.U, a.Nc, s[k].y, un);
 #pragma unroll
                 for (int v = 0; v < 4; v++) {
                     // GaussGreen.cpp:25-28: uf = u_CL If + u_CR (1 - If); +uf Af n into CL,
@@ -330,18 +334,17 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
                     const T d = gx * ro[k][0] + gy * ro[k][1];   // Limiter.cpp:50-51
                     T pf = T(1);
                     if (a.limiter == LIM_BJ) {                   // Limiter.cpp:67-71
-                        pf = (d > eps) ? fmin(T(1), (umax[v] - u[v]) / d) : pf;
-                        pf = (d < -eps) ? fmin(T(1), (umin[v] - u[v]) / d) : pf;
+                        // one division: the numerator is picked by the sign of d
+                        if (d > eps || d < -eps) pf = fmin(T(1), ((d > eps) ? umax[v] - u[v] : umin[v] - u[v]) / d);
                     } else {
-                        pf = (d > eps) ? venkat(umax[v] - u[v], d, e2) : pf;
-                        pf = (d < -eps) ? venkat(umin[v] - u[v], d, e2) : pf;
+                        if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
                     }
                     phi = fmin(phi, pf);                         // Limiter.cpp:73-74
                 }
                 out[2 * v] = phi * gx;
                 out[2 * v + 1] = phi * gy;
             }
-            st_grad(a.phiG, c, out);
+            st_grad(a.phiG, a.Nc, c, out);
             if (a.time_mode != TM_FIXED) dtc = (double) (T(1) / (iv * lam));
         }
     }
@@ -376,8 +379,8 @@ __global__ void __launch_bounds__(256) pass2_kernel(const StepArgs<T> a) {
         for (int k = 0; k < W; k++) s[k] = __ldg(a.slot + (size_t) k * a.Nc + c);
         if (s[0].y >= 0) {
             T u[4], pg[8];
-            ld_cell(a.U, c, u);
-            ld_grad(a.phiG, c, pg);
+            ld_cell(a.U, a.Nc, c, u);
+            ld_grad(a.phiG, a.Nc, c, pg);
             const T iv = __ldg(a.iv + c);
             T R[4], Rc[4];
 #pragma unroll
@@ -394,7 +397,7 @@ __global__ void __launch_bounds__(256) pass2_kernel(const StepArgs<T> a) {
                 const T ro0 = isL ? g.rLx : g.rRx, ro1 = isL ? g.rLy : g.rRy;
                 const T rn0 = isL ? g.rRx : g.rLx, rn1 = isL ? g.rRy : g.rLy;
                 T un[4], uo[4], uq[4];
-                ld_cell(a.U, s[k].y, un);
+                ld_cell(a.U, a.Nc, s[k].y, un);
                 // MUSCL (Flux.cpp:83-87): U + phi grad U . r on each side.  A ghost
                 // neighbour carries -grad and the same phi as this cell (BoundaryConditions/
                 // Base.cpp:29-53) with r_R = -r_L (Domain.cpp:84-88), so its increment is this
@@ -408,7 +411,7 @@ __global__ void __launch_bounds__(256) pass2_kernel(const StepArgs<T> a) {
                     }
                 } else {
                     T pn[8];
-                    ld_grad(a.phiG, s[k].y, pn);
+                    ld_grad(a.phiG, a.Nc, s[k].y, pn);
 #pragma unroll
                     for (int v = 0; v < 4; v++) {
                         uo[v] = u[v] + (pg[2 * v] * ro0 + pg[2 * v + 1] * ro1);
@@ -442,7 +445,7 @@ __global__ void __launch_bounds__(256) pass2_kernel(const StepArgs<T> a) {
                 if (v == 0) r2 = (double) Rv * (double) Rv;
                 bad |= !isfinite(un_[v]);
             }
-            st_cell(a.Unew, c, un_);
+            st_cell(a.Unew, a.Nc, c, un_);
             // Ghost refresh (update_BC_cells, Euler.cpp:96 and :138-142): this cell is the
             // only interior neighbour of each of its ghosts.
 #pragma unroll
@@ -455,7 +458,7 @@ __global__ void __launch_bounds__(256) pass2_kernel(const StepArgs<T> a) {
                 ld_geo(a.geo, f, g);
                 T ug[4];
                 ghost_state(a.bc.type[b], un_, g.nx, g.ny, a.gma, a.bc.UBC[b], a.bc.QBC[b], ug);
-                st_cell(a.Unew, s[k].y, ug);
+                st_cell(a.Unew, a.Nc, s[k].y, ug);
             }
         }
     }
@@ -605,58 +608,68 @@ __global__ void fill_kernel(int Nc, Cell4<T>* __restrict__ U, double u0, double 
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= Nc) return;
     const T u[4] = {T(u0), T(u1), T(u2), T(u3)};
-    st_cell(U, i, u);
+    st_cell(U, Nc, i, u);
 }
 
 // Euler::update_BC_cells over all boundary faces (used by initialise and upload).
+// fc holds the faces' cells in the device's internal numbering.
 template <class T>
-__global__ void bc_cells_kernel(int Nf, int F_BC, const int* __restrict__ fc_con, const FaceGeo<T>* __restrict__ geo,
+__global__ void bc_cells_kernel(int Nc, int Nf, int F_BC, const int* __restrict__ fc, const FaceGeo<double>* __restrict__ geo,
                                 Cell4<T>* __restrict__ U, T gma, const BCTable bc) {
     const int f = F_BC + blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= Nf) return;
     const int b = bc_of_face(bc, f);
     T uc[4], ug[4];
-    ld_cell(U, fc_con[2 * f], uc);
-    FaceGeo<T> g;
-    ld_geo(geo, f, g);
-    ghost_state(bc.type[b], uc, g.nx, g.ny, gma, bc.UBC[b], bc.QBC[b], ug);
-    st_cell(U, fc_con[2 * f + 1], ug);
+    ld_cell(U, Nc, fc[2 * f], uc);
+    const FaceGeo<double> g = geo[f];
+    ghost_state(bc.type[b], uc, T(g.nx), T(g.ny), gma, bc.UBC[b], bc.QBC[b], ug);
+    st_cell(U, Nc, fc[2 * f + 1], ug);
 }
 
 // Euler::compute_prims (src/Base/Euler.cpp:115-136), or a plain copy of U; variable-major
-// double output.
+// double output in the input numbering (perm[internal] = input index).
 template <class T>
-__global__ void out_kernel(int Nc, const Cell4<T>* __restrict__ U, double gma, int prims, double* __restrict__ out) {
+__global__ void out_kernel(int Nc, const Cell4<T>* __restrict__ U, const int* __restrict__ perm, double gma,
+                           int prims, double* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= Nc) return;
     T t[4];
-    ld_cell(U, i, t);
+    ld_cell(U, Nc, i, t);
+    const size_t j = perm[i];
     const double u0 = t[0], u1 = t[1], u2 = t[2], u3 = t[3];
     if (!prims) {
-        out[i] = u0; out[(size_t) Nc + i] = u1; out[2 * (size_t) Nc + i] = u2; out[3 * (size_t) Nc + i] = u3;
+        out[j] = u0; out[(size_t) Nc + j] = u1; out[2 * (size_t) Nc + j] = u2; out[3 * (size_t) Nc + j] = u3;
         return;
     }
     const double q0 = u0, q1 = u1 / u0, q2 = u2 / u0;
     const double gmo = gma - 1;
     const double q3 = gmo * (u3 - 0.5 * q0 * (q1 * q1 + q2 * q2));
-    out[i] = q0; out[(size_t) Nc + i] = q1; out[2 * (size_t) Nc + i] = q2; out[3 * (size_t) Nc + i] = q3;
+    out[j] = q0; out[(size_t) Nc + j] = q1; out[2 * (size_t) Nc + j] = q2; out[3 * (size_t) Nc + j] = q3;
 }
 
 template <class T>
-__global__ void in_kernel(int Nc, const double* __restrict__ in, Cell4<T>* __restrict__ U) {
+__global__ void in_kernel(int Nc, const double* __restrict__ in, const int* __restrict__ perm, Cell4<T>* __restrict__ U) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= Nc) return;
-    const T u[4] = {T(in[i]), T(in[(size_t) Nc + i]), T(in[2 * (size_t) Nc + i]), T(in[3 * (size_t) Nc + i])};
-    st_cell(U, i, u);
+    const size_t j = perm[i];
+    const T u[4] = {T(in[j]), T(in[(size_t) Nc + j]), T(in[2 * (size_t) Nc + j]), T(in[3 * (size_t) Nc + j])};
+    st_cell(U, Nc, i, u);
+}
+
+// dst[i] = src[perm[i]]
+__global__ void permute_kernel(int n, const double* __restrict__ src, const int* __restrict__ perm,
+                               double* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[perm[i]];
 }
 
 template <class T>
-__global__ void wall_cp_kernel(int F1, int F2, const int* __restrict__ fc_con, const Cell4<T>* __restrict__ U,
+__global__ void wall_cp_kernel(int Nc, int F1, int F2, const int* __restrict__ fc_con, const Cell4<T>* __restrict__ U,
                                double gma, double p_inf, double qinf, double* __restrict__ out) {
     const int f = F1 + blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= F2) return;
     T t[4];
-    ld_cell(U, fc_con[2 * f], t);
+    ld_cell(U, Nc, fc_con[2 * f], t);
     const double r = t[0], ru = t[1], rv = t[2], E = t[3];
     const double p = (gma - 1) * (E - 0.5 * (ru * ru + rv * rv) / r);
     out[f - F1] = (p - p_inf) / qinf;

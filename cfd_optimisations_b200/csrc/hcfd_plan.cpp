@@ -1,0 +1,235 @@
+// Host-side execution plan of the tiled step kernels.
+//
+// The device keeps cells in an internal order (a Morton curve over the cell centres by
+// default, so that consecutive cells are close in space whatever the input numbering) and
+// cuts that order into tiles of B consecutive cells.  For each tile the plan lists
+//   - its halo: cells outside the tile that neighbour one of its real cells;
+//   - its face entries: every face with a real tile cell on either side, once per tile,
+//     with the local indices (tile cells 0..B-1, halo cells B..) of both cells, the flux
+//     slots the entry feeds (local cell * W + position of the face in that cell's face
+//     list), and the boundary-condition index of boundary faces;
+//   - per tile cell and face position: the local entry index and the side of the cell.
+// A cell's face positions follow its faces in increasing face index (the order of the
+// reference's cell->face table, src/Mesh.cpp:88-117), so per-cell sums formed slot by
+// slot add in the reference's order.
+#include "hcfd_internal.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+namespace hcfd {
+
+namespace {
+unsigned long long spread16(unsigned long long x) {
+    x &= 0xFFFFULL;
+    x = (x | (x << 8)) & 0x00FF00FFULL;
+    x = (x | (x << 4)) & 0x0F0F0F0FULL;
+    x = (x | (x << 2)) & 0x33333333ULL;
+    x = (x | (x << 1)) & 0x55555555ULL;
+    return x;
+}
+}  // namespace
+
+std::vector<int> morton_order(const hcfd_mesh_view& v) {
+    double lo[2] = {1e300, 1e300}, hi[2] = {-1e300, -1e300};
+    for (int i = 0; i < v.Nn; i++)
+        for (int d = 0; d < 2; d++) { lo[d] = std::min(lo[d], v.nodes[2 * i + d]); hi[d] = std::max(hi[d], v.nodes[2 * i + d]); }
+    std::vector<unsigned int> key(v.Nc);
+    for (int c = 0; c < v.Nc; c++) {
+        double x[2] = {0, 0};
+        const int b = v.cn_off[c], e = v.cn_off[c + 1];
+        for (int k = b; k < e; k++)
+            for (int d = 0; d < 2; d++) x[d] += v.nodes[2 * v.cn_con[k] + d];
+        unsigned long long q[2];
+        for (int d = 0; d < 2; d++) {
+            double t = (hi[d] > lo[d]) ? (x[d] / (e - b) - lo[d]) / (hi[d] - lo[d]) : 0.0;
+            t = std::min(std::max(t, 0.0), 1.0);
+            q[d] = (unsigned long long) (t * 65535.0);
+        }
+        key[c] = (unsigned int) (spread16(q[0]) | (spread16(q[1]) << 1));
+    }
+    std::vector<int> perm(v.Nc);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+    return perm;
+}
+
+int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, const std::vector<int>& cf_con,
+                    const std::vector<char>& ghost, const std::vector<int>& perm, int F_BC,
+                    const std::vector<int>& bc_first, int B, int W, TilePlan& P) {
+    const int Nc = v.Nc;
+    P.B = B;
+    P.W = W;
+    P.Wp = W <= 4 ? 4 : 8;
+    P.ntiles = (Nc + B - 1) / B;
+    std::vector<int> iperm(Nc);
+    for (int i = 0; i < Nc; i++) iperm[perm[i]] = i;
+    auto bc_of = [&](int f) {
+        int k = 0;
+        while (k + 1 < (int) bc_first.size() && f >= bc_first[k + 1]) k++;
+        return k;
+    };
+    // position of face f in user cell u's face list
+    auto pos_in = [&](int u, int f) {
+        for (int j = cf_off[u]; j < cf_off[u + 1]; j++) if (cf_con[j] == f) return j - cf_off[u];
+        return -1;
+    };
+    P.foff.assign(P.ntiles + 1, 0);
+    P.hoff.assign(P.ntiles + 1, 0);
+    P.cslot.assign((size_t) P.ntiles * B * P.Wp, (short) -1);
+    P.efid.clear();
+    P.meta.clear();
+    P.halo.clear();
+    std::vector<int> fstamp(v.Nf, -1), fentry(v.Nf, 0), hstamp(Nc, -1), hidx(Nc, 0);
+    P.Hmax = 0;
+    P.Fmax = 0;
+    for (int t = 0; t < P.ntiles; t++) {
+        const int base = t * B, nb = std::min(B, Nc - base);
+        const int h0 = (int) P.halo.size();
+        const int e0 = (int) P.efid.size();
+        auto local = [&](int ci) -> int {   // ci: internal index
+            if (ci >= base && ci < base + nb) return ci - base;
+            if (hstamp[ci] != t) {
+                hstamp[ci] = t;
+                hidx[ci] = (int) P.halo.size() - h0;
+                P.halo.push_back(ci);
+            }
+            return B + hidx[ci];
+        };
+        for (int c = 0; c < nb; c++) {
+            const int ci = base + c, u = perm[ci];
+            if (ghost[u]) continue;
+            for (int j = cf_off[u], k = 0; j < cf_off[u + 1]; j++, k++) {
+                const int f = cf_con[j];
+                const int uL = v.fc_con[2 * f], uR = v.fc_con[2 * f + 1];
+                if (fstamp[f] != t) {
+                    fstamp[f] = t;
+                    fentry[f] = (int) P.efid.size() - e0;
+                    const int iL = iperm[uL], iR = iperm[uR];
+                    const int la = local(iL), lb = local(iR);
+                    const bool inL = la < B && !ghost[uL], inR = lb < B && !ghost[uR];
+                    short m[8] = {(short) la, (short) lb,
+                                  (short) (inL ? la * W + pos_in(uL, f) : -1),
+                                  (short) (inR ? lb * W + pos_in(uR, f) : -1),
+                                  (short) (f >= F_BC ? bc_of(f) : -1), 0, 0, 0};
+                    P.efid.push_back(f);
+                    P.meta.insert(P.meta.end(), m, m + 8);
+                }
+                const int e = fentry[f];
+                if (e > 16383) return fail(HCFD_EINVAL, "tile plan: too many faces in one tile");
+                P.cslot[((size_t) t * B + c) * P.Wp + k] = (short) ((e << 1) | (uR == u ? 1 : 0));
+            }
+        }
+        // pad the entries to a multiple of 4 so every per-tile block is a multiple of 16 B
+        while (((int) P.efid.size() - e0) % 4) {
+            short m[8] = {0, 0, -1, -1, -1, 0, 0, 0};
+            P.efid.push_back(-1);
+            P.meta.insert(P.meta.end(), m, m + 8);
+        }
+        P.foff[t + 1] = (int) P.efid.size();
+        P.hoff[t + 1] = (int) P.halo.size();
+        P.Hmax = std::max(P.Hmax, (int) P.halo.size() - h0);
+        P.Fmax = std::max(P.Fmax, (int) P.efid.size() - e0);
+        if (B + P.Hmax > 32767) return fail(HCFD_EINVAL, "tile plan: halo too large");
+    }
+    return HCFD_OK;
+}
+
+}  // namespace hcfd
+
+// ---------------------------------------------------------------------------------------
+// Host check of every index the tiled kernels derive from a plan.
+
+extern "C" int hcfd_plan_check(const hcfd_mesh_view* v, int tile, int keep_numbering, long long* info) {
+    using namespace hcfd;
+    clear_error();
+    if (!v) return fail(HCFD_EINVAL, "plan_check: null mesh");
+    int rc = validate_view(*v);
+    if (rc != HCFD_OK) return rc;
+    const int Nc = v->Nc, Nf = v->Nf;
+    const int F_BC = v->coloff[v->Ncol - v->NBCcol];
+    std::vector<int> cf_off, cf_con;
+    build_cf(Nc, Nf, v->fc_con, cf_off, cf_con);
+    std::vector<char> ghost(Nc, 0);
+    for (int f = F_BC; f < Nf; f++) ghost[v->fc_con[2 * f + 1]] = 1;
+    int maxdeg = 0;
+    for (int c = 0; c < Nc; c++) if (!ghost[c]) maxdeg = std::max(maxdeg, cf_off[c + 1] - cf_off[c]);
+    const int W = maxdeg <= 3 ? 3 : maxdeg <= 4 ? 4 : 8;
+    std::vector<int> perm;
+    if (keep_numbering) { perm.resize(Nc); std::iota(perm.begin(), perm.end(), 0); }
+    else perm = morton_order(*v);
+    std::vector<int> bc_first;
+    for (int col = v->Ncol - v->NBCcol; col < v->Ncol; col++) bc_first.push_back(v->coloff[col]);
+    const int B = tile ? tile : 256;
+    TilePlan P;
+    rc = build_tile_plan(*v, cf_off, cf_con, ghost, perm, F_BC, bc_first, B, W, P);
+    if (rc != HCFD_OK) return rc;
+    std::vector<int> iperm(Nc);
+    for (int i = 0; i < Nc; i++) iperm[perm[i]] = i;
+    auto bad = [&](const char* what, int t) {
+        return fail(HCFD_EINVAL, std::string("plan_check: ") + what + " (tile " + std::to_string(t) + ")");
+    };
+    const int E = (int) P.efid.size();
+    if (P.foff[0] != 0 || P.foff[P.ntiles] != E || P.hoff[0] != 0 || P.hoff[P.ntiles] != (int) P.halo.size())
+        return bad("offset arrays do not span", -1);
+    long long cut = 0, internal = 0;
+    std::vector<int> written(B * W);
+    for (int t = 0; t < P.ntiles; t++) {
+        const int base = t * B, nb = std::min(B, Nc - base);
+        const int f0 = P.foff[t], nf = P.foff[t + 1] - f0, h0 = P.hoff[t], nh = P.hoff[t + 1] - h0;
+        if (nf < 0 || nh < 0 || nf % 4 || nf > P.Fmax || nh > P.Hmax) return bad("entry or halo count", t);
+        // bulk-copy sizes and offsets: multiples of 16 bytes (float and double layouts)
+        if ((nb * 16) % 16 || (f0 * 32) % 16 || (f0 * 16) % 16 || (base * 16) % 16) return bad("bulk alignment", t);
+        for (int h = 0; h < nh; h++) {
+            const int ci = P.halo[h0 + h];
+            if (ci < 0 || ci >= Nc || (ci >= base && ci < base + nb)) return bad("halo id", t);
+        }
+        auto cell_of = [&](int l) { return l < B ? base + l : P.halo[h0 + l - B]; };
+        std::fill(written.begin(), written.end(), 0);
+        for (int e = 0; e < nf; e++) {
+            const short* m = &P.meta[8 * (size_t) (f0 + e)];
+            const int la = m[0], lb = m[1], sL = m[2], sR = m[3], bc = m[4];
+            const int f = P.efid[f0 + e];
+            const bool okl = (la < nb) || (la >= B && la < B + nh);
+            const bool okr = (lb < nb) || (lb >= B && lb < B + nh);
+            if (la < 0 || lb < 0 || !okl || !okr) return bad("local cell index", t);
+            if (f < 0) {
+                if (sL != -1 || sR != -1) return bad("padding entry feeds a slot", t);
+                continue;
+            }
+            if (cell_of(la) != iperm[v->fc_con[2 * f]] || cell_of(lb) != iperm[v->fc_con[2 * f + 1]])
+                return bad("entry cells differ from the face's cells", t);
+            if ((f >= F_BC) != (bc >= 0) || bc >= (int) bc_first.size()) return bad("boundary index", t);
+            if (sL < -1 || sL >= nb * W || sR < -1 || sR >= nb * W) return bad("slot range", t);
+            if (sL >= 0) { if (sL / W != la) return bad("left slot owner", t); written[sL]++; }
+            if (sR >= 0) { if (sR / W != lb) return bad("right slot owner", t); written[sR]++; }
+            if (sL >= 0 && sR >= 0) internal++; else cut++;
+        }
+        for (int c = 0; c < nb; c++) {
+            const int u = perm[base + c];
+            const short* cs = &P.cslot[((size_t) t * B + c) * P.Wp];
+            const int deg = ghost[u] ? 0 : cf_off[u + 1] - cf_off[u];
+            for (int k = 0; k < P.Wp; k++) {
+                if (k >= deg) {
+                    if (cs[k] != -1) return bad("slot beyond the cell's faces", t);
+                    if (k < W && written[c * W + k]) return bad("unused slot written", t);
+                    continue;
+                }
+                if (cs[k] < 0) return bad("missing slot", t);
+                const int e = cs[k] >> 1, side = cs[k] & 1;
+                if (e >= nf) return bad("slot entry out of range", t);
+                const short* m = &P.meta[8 * (size_t) (f0 + e)];
+                if ((side ? m[1] : m[0]) != c) return bad("slot side", t);
+                if ((side ? m[3] : m[2]) != c * W + k) return bad("slot position", t);
+                if (P.efid[f0 + e] != cf_con[cf_off[u] + k]) return bad("slot face order", t);
+                if (written[c * W + k] != 1) return bad("slot not written exactly once", t);
+            }
+        }
+    }
+    if (info) {
+        info[0] = P.ntiles; info[1] = P.Hmax; info[2] = P.Fmax; info[3] = E;
+        info[4] = internal; info[5] = cut; info[6] = W; info[7] = (long long) P.halo.size();
+    }
+    return HCFD_OK;
+}

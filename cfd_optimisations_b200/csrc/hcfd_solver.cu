@@ -1,14 +1,22 @@
 // Solver handle of the B200 solver: device memory, the per-handle stream, launches of the
 // step kernels and the C ABI of include/hcfd_gpu.h for one mesh.
+//
+// Device numbering.  Cells live on the device in an internal order: the Morton order of the
+// cell centres by default (so that consecutive cells are neighbours in space, whatever the
+// input numbering), or the input order with keep_numbering.  Faces keep their input
+// numbers, and each cell's faces are visited in increasing face number, so the internal
+// order changes where data sits, never the arithmetic.  State crosses the ABI in the input
+// numbering.
 #include "hcfd_internal.hpp"
 #include "hcfd_kernels.cuh"
+#include "hcfd_tile.cuh"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
-#include <type_traits>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using hcfd::fail;
@@ -46,20 +54,20 @@ void prim_to_cons(const double* q, double gma, double* u) {
 }  // namespace
 
 struct hcfd_solver {
-    int device = 0;
+    int device = 0, nsm = 0;
     cudaStream_t stream = nullptr;
     hcfd_params prm{};
     int Nc = 0, Nf = 0, Nn = 0, Ncol = 0, NBC = 0, F_BC = 0, Nreal = 0, W = 0;
     std::vector<int> coloff, coltag;
     bool bcs_set = false, initialised = false;
     hcfd::BCTable bc{};
-    // device buffers
-    int* d_fc = nullptr;                 // fc_con [2 Nf]
-    int2* d_slot = nullptr;              // [W][Nc]
-    void* d_geo = nullptr;               // FaceGeo<T> [Nf]
-    hcfd::FaceGeo<double>* d_geo64 = nullptr;
+    // device buffers (cells in internal order)
+    int* d_fc = nullptr;                 // fc_con in internal cell numbers [2 Nf]
+    int* d_perm = nullptr;               // internal -> input cell number
+    int2* d_slot = nullptr;              // per-cell kernels: [W][Nc]
+    hcfd::FaceGeo<double>* d_geo64 = nullptr;   // [Nf], input face order
+    void* d_geoT = nullptr;              // per-cell kernels in float: FaceGeo<float> [Nf]
     void* d_iv = nullptr;                // T [Nc]
-    double* d_iv64 = nullptr;
     void* d_U[2] = {nullptr, nullptr};   // Cell4<T> [Nc]
     void* d_phiG = nullptr;              // Grad8<T> [Nc]
     double* d_io = nullptr;              // 4 Nc doubles staging for upload/download
@@ -67,9 +75,20 @@ struct hcfd_solver {
     unsigned long long* d_dtmin = nullptr;   // [2]
     double* d_partial = nullptr;
     unsigned int* d_counter = nullptr;
+    unsigned int* d_err = nullptr;
     hcfd::StepStats* d_stats = nullptr;
+    // tiled kernels
+    hcfd::TilePlan plan;
+    void* d_tgeo = nullptr;              // FaceGeo<T> [entries]
+    short* d_tmeta = nullptr;
+    int *d_foff = nullptr, *d_hoff = nullptr, *d_halo = nullptr;
+    short* d_cslot = nullptr;
+    size_t smem1 = 0, smem2 = 0;
+    int grid1 = 0, grid2 = 0;
+    bool tiled = false;
     int cur = 0;                         // which of d_U holds the state
     int block = 256;
+    int partial_len = 0;
     // profiling
     bool prof = false;
     std::vector<cudaEvent_t> ev1, ev2;   // start/stop pairs per launch
@@ -87,8 +106,9 @@ void free_all(hcfd_solver* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto e : s->ev1) cudaEventDestroy(e);
     for (auto e : s->ev2) cudaEventDestroy(e);
-    void* ptrs[] = {s->d_fc, s->d_slot, s->d_geo, s->d_geo64, s->d_iv, s->d_iv64, s->d_U[0], s->d_U[1],
-                    s->d_phiG, s->d_io, s->d_cp, s->d_dtmin, s->d_partial, s->d_counter, s->d_stats};
+    void* ptrs[] = {s->d_fc, s->d_perm, s->d_slot, s->d_geo64, s->d_geoT, s->d_iv, s->d_U[0], s->d_U[1],
+                    s->d_phiG, s->d_io, s->d_cp, s->d_dtmin, s->d_partial, s->d_counter, s->d_err, s->d_stats,
+                    s->d_tgeo, s->d_tmeta, s->d_foff, s->d_hoff, s->d_halo, s->d_cslot};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (s->stream) cudaStreamDestroy(s->stream);
 }
@@ -99,7 +119,7 @@ hcfd::StepArgs<T> step_args(hcfd_solver* s, int time_mode, double dt_or_cfl) {
     a.U = (const hcfd::Cell4<T>*) s->d_U[s->cur];
     a.Unew = (hcfd::Cell4<T>*) s->d_U[1 - s->cur];
     a.phiG = (hcfd::Grad8<T>*) s->d_phiG;
-    a.geo = (const hcfd::FaceGeo<T>*) s->d_geo;
+    a.geo = std::is_same<T, double>::value ? (const hcfd::FaceGeo<T>*) s->d_geo64 : (const hcfd::FaceGeo<T>*) s->d_geoT;
     a.slot = s->d_slot;
     a.iv = (const T*) s->d_iv;
     a.dtmin = s->d_dtmin + s->cur;
@@ -118,22 +138,65 @@ hcfd::StepArgs<T> step_args(hcfd_solver* s, int time_mode, double dt_or_cfl) {
     return a;
 }
 
+template <class T>
+hcfd::TileArgs<T> tile_args(hcfd_solver* s, int time_mode, double dt_or_cfl) {
+    hcfd::TileArgs<T> a;
+    a.s = step_args<T>(s, time_mode, dt_or_cfl);
+    a.tgeo = (const T*) s->d_tgeo;
+    a.tmeta = s->d_tmeta;
+    a.foff = s->d_foff;
+    a.hoff = s->d_hoff;
+    a.halo = s->d_halo;
+    a.cslot = s->d_cslot;
+    a.ntiles = s->plan.ntiles;
+    a.B = s->plan.B;
+    a.Wp = s->plan.Wp;
+    a.Hmax = s->plan.Hmax;
+    a.Fmax = s->plan.Fmax;
+    a.err = s->d_err;
+    return a;
+}
+
+struct Ev {
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+
+int prof_begin(hcfd_solver* s, Ev& e) {
+    if (!s->prof) return HCFD_OK;
+    CK(cudaEventCreate(&e.a));
+    CK(cudaEventCreate(&e.b));
+    CK(cudaEventRecord(e.a, s->stream));
+    return HCFD_OK;
+}
+int prof_end(hcfd_solver* s, Ev& e, std::vector<cudaEvent_t>& into) {
+    if (!s->prof) return HCFD_OK;
+    CK(cudaEventRecord(e.b, s->stream));
+    into.push_back(e.a);
+    into.push_back(e.b);
+    return HCFD_OK;
+}
+
 template <class T, int W>
 int launch_step(hcfd_solver* s, int time_mode, double dt_or_cfl) {
-    const int grid = nblk(s->Nc, s->block);
-    hcfd::StepArgs<T> a = step_args<T>(s, time_mode, dt_or_cfl);
-    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
-    if (s->prof) {
-        CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1)); CK(cudaEventCreate(&e2)); CK(cudaEventCreate(&e3));
-        CK(cudaEventRecord(e0, s->stream));
-    }
-    hcfd::pass1_kernel<T, W><<<grid, s->block, 0, s->stream>>>(a);
-    if (s->prof) { CK(cudaEventRecord(e1, s->stream)); CK(cudaEventRecord(e2, s->stream)); }
-    hcfd::pass2_kernel<T, W, std::is_same<T, float>::value><<<grid, s->block, 0, s->stream>>>(a);
-    if (s->prof) {
-        CK(cudaEventRecord(e3, s->stream));
-        s->ev1.push_back(e0); s->ev1.push_back(e1);
-        s->ev2.push_back(e2); s->ev2.push_back(e3);
+    Ev e1, e2;
+    int rc;
+    if (s->tiled) {
+        hcfd::TileArgs<T> a = tile_args<T>(s, time_mode, dt_or_cfl);
+        if ((rc = prof_begin(s, e1))) return rc;
+        hcfd::tile_pass1_kernel<T, W><<<s->grid1, s->block + 32, s->smem1, s->stream>>>(a);
+        if ((rc = prof_end(s, e1, s->ev1))) return rc;
+        if ((rc = prof_begin(s, e2))) return rc;
+        hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value><<<s->grid2, s->block + 32, s->smem2, s->stream>>>(a);
+        if ((rc = prof_end(s, e2, s->ev2))) return rc;
+    } else {
+        const int grid = nblk(s->Nc, s->block);
+        hcfd::StepArgs<T> a = step_args<T>(s, time_mode, dt_or_cfl);
+        if ((rc = prof_begin(s, e1))) return rc;
+        hcfd::pass1_kernel<T, W><<<grid, s->block, 0, s->stream>>>(a);
+        if ((rc = prof_end(s, e1, s->ev1))) return rc;
+        if ((rc = prof_begin(s, e2))) return rc;
+        hcfd::pass2_kernel<T, W, std::is_same<T, float>::value><<<grid, s->block, 0, s->stream>>>(a);
+        if ((rc = prof_end(s, e2, s->ev2))) return rc;
     }
     CK(cudaGetLastError());
     s->cur = 1 - s->cur;
@@ -149,13 +212,44 @@ int launch_step_w(hcfd_solver* s, int time_mode, double dt_or_cfl) {
     }
 }
 
+// Shared-memory opt-in and persistent grid size of the tiled kernels for one (T, W).
+template <class T, int W>
+int setup_tiled_w(hcfd_solver* s) {
+    const hcfd::TilePlan& P = s->plan;
+    s->smem1 = hcfd::TileSmem<T>(P.B, P.Hmax, P.Fmax, W, P.Wp, false).total;
+    s->smem2 = hcfd::TileSmem<T>(P.B, P.Hmax, P.Fmax, W, P.Wp, true).total;
+    int maxsm = 0;
+    CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
+    if ((int) s->smem2 > maxsm || (int) s->smem1 > maxsm) return fail(HCFD_EINVAL, "tile does not fit in shared memory");
+    CK(cudaFuncSetAttribute(hcfd::tile_pass1_kernel<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) s->smem1));
+    CK(cudaFuncSetAttribute(hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int) s->smem2));
+    int b1 = 0, b2 = 0;
+    // blocks of the tiled kernels: `block` compute threads + one producer warp
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, hcfd::tile_pass1_kernel<T, W>, s->block + 32, s->smem1));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value>,
+                                                     s->block + 32, s->smem2));
+    if (b1 < 1 || b2 < 1) return fail(HCFD_EINVAL, "tiled kernels cannot be resident");
+    s->grid1 = std::min(P.ntiles, b1 * s->nsm);
+    s->grid2 = std::min(P.ntiles, b2 * s->nsm);
+    return HCFD_OK;
+}
+
+template <class T>
+int setup_tiled(hcfd_solver* s) {
+    switch (s->W) {
+    case 3: return setup_tiled_w<T, 3>(s);
+    case 4: return setup_tiled_w<T, 4>(s);
+    default: return setup_tiled_w<T, 8>(s);
+    }
+}
+
 template <class T>
 int refresh_ghosts(hcfd_solver* s) {
     const int nbf = s->Nf - s->F_BC;
     if (nbf > 0)
         hcfd::bc_cells_kernel<T><<<nblk(nbf, 256), 256, 0, s->stream>>>(
-            s->Nf, s->F_BC, s->d_fc, (const hcfd::FaceGeo<T>*) s->d_geo, (hcfd::Cell4<T>*) s->d_U[s->cur],
-            T(s->prm.gma), s->bc);
+            s->Nc, s->Nf, s->F_BC, s->d_fc, s->d_geo64, (hcfd::Cell4<T>*) s->d_U[s->cur], T(s->prm.gma), s->bc);
     CK(cudaGetLastError());
     return HCFD_OK;
 }
@@ -168,7 +262,9 @@ int check_handle(hcfd_solver* s) {
 
 int read_stats(hcfd_solver* s, hcfd_step_stats* out) {
     hcfd::StepStats st;
+    unsigned int err = 0;
     CK(cudaMemcpyAsync(&st, s->d_stats, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(&err, s->d_err, sizeof(err), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     if (out) {
         out->dt = st.dt_last;
@@ -177,6 +273,7 @@ int read_stats(hcfd_solver* s, hcfd_step_stats* out) {
         out->steps = st.steps;
         out->nonfinite = st.nonfinite;
     }
+    if (err) return fail(HCFD_ETIMEOUT, "a bounded device wait gave up (tile staging did not complete)");
     return st.nonfinite ? fail(HCFD_ENONFINITE, "a step produced a NaN or Inf") : HCFD_OK;
 }
 
@@ -190,10 +287,12 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
     *out = nullptr;
     int rc = hcfd::validate_view(*mv);
     if (rc != HCFD_OK) return rc;
-    hcfd_params p{1.4, HCFD_LIMITER_BJ, 5.0, HCFD_FP64, 0};
+    hcfd_params p{1.4, HCFD_LIMITER_BJ, 5.0, HCFD_FP64, 0, HCFD_KERNEL_TILED, 0, 0};
     if (prm) p = *prm;
     if (!(p.gma > 1.0) || (p.limiter != HCFD_LIMITER_BJ && p.limiter != HCFD_LIMITER_VENKAT) ||
-        (p.precision != HCFD_FP64 && p.precision != HCFD_FP32) || p.block < 0 || p.block > 1024 || (p.block % 32))
+        (p.precision != HCFD_FP64 && p.precision != HCFD_FP32) || p.block < 0 || p.block > 1024 || (p.block % 32) ||
+        (p.kernel != HCFD_KERNEL_TILED && p.kernel != HCFD_KERNEL_CELL) || p.tile < 0 || p.tile > 512 || (p.tile % 32) ||
+        (p.kernel == HCFD_KERNEL_TILED && p.block > 256))
         return fail(HCFD_EINVAL, "gpu_create: bad parameters");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -201,6 +300,7 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
 
     auto s = std::make_unique<hcfd_solver>();
     CK(cudaGetDevice(&s->device));
+    CK(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, s->device));
     s->prm = p;
     s->block = p.block ? p.block : 256;
     s->Nc = mv->Nc; s->Nf = mv->Nf; s->Nn = mv->Nn; s->Ncol = mv->Ncol; s->NBC = mv->NBCcol;
@@ -208,29 +308,51 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
     s->coltag.assign(mv->coltag, mv->coltag + mv->Ncol);
     s->F_BC = s->coloff[s->Ncol - s->NBC];
     if (s->NBC > hcfd::MAXBC) return fail(HCFD_EINVAL, "gpu_create: more than 16 boundary colours");
+    const int Nc = s->Nc, Nf = s->Nf;
 
-    // Cell -> face slots (ELL, slot-major) from the reference's CSR table: faces of each
-    // real cell in increasing face index; ghost cells get no slots.
+    // Host-side topology: cell->face table, ghosts, internal order.
     std::vector<int> cf_off, cf_con;
-    hcfd::build_cf(s->Nc, s->Nf, mv->fc_con, cf_off, cf_con);
-    std::vector<char> ghost(s->Nc, 0);
-    for (int f = s->F_BC; f < s->Nf; f++) ghost[mv->fc_con[2 * f + 1]] = 1;
+    hcfd::build_cf(Nc, Nf, mv->fc_con, cf_off, cf_con);
+    std::vector<char> ghost(Nc, 0);
+    for (int f = s->F_BC; f < Nf; f++) ghost[mv->fc_con[2 * f + 1]] = 1;
     int maxdeg = 0;
-    for (int c = 0; c < s->Nc; c++) {
+    for (int c = 0; c < Nc; c++) {
         if (ghost[c]) continue;
         s->Nreal++;
         maxdeg = std::max(maxdeg, cf_off[c + 1] - cf_off[c]);
     }
     if (maxdeg > 8) return fail(HCFD_EINVAL, "gpu_create: a cell has more than 8 faces");
     s->W = maxdeg <= 3 ? 3 : maxdeg <= 4 ? 4 : 8;
-    std::vector<int2> slot((size_t) s->W * s->Nc, make_int2(-1, -1));
-    for (int c = 0; c < s->Nc; c++) {
-        if (ghost[c]) continue;
-        int k = 0;
-        for (int j = cf_off[c]; j < cf_off[c + 1]; j++, k++) {
-            const int f = cf_con[j];
-            const int L = mv->fc_con[2 * f], R = mv->fc_con[2 * f + 1];
-            slot[(size_t) k * s->Nc + c] = (L == c) ? make_int2(f, R) : make_int2(~f, L);
+    std::vector<int> perm;
+    if (p.keep_numbering) { perm.resize(Nc); for (int i = 0; i < Nc; i++) perm[i] = i; }
+    else perm = hcfd::morton_order(*mv);
+    std::vector<int> iperm(Nc);
+    for (int i = 0; i < Nc; i++) iperm[perm[i]] = i;
+    std::vector<int> fc_int(2 * (size_t) Nf);
+    for (size_t k = 0; k < fc_int.size(); k++) fc_int[k] = iperm[mv->fc_con[k]];
+    std::vector<int> bc_first;
+    for (int col = s->Ncol - s->NBC; col < s->Ncol; col++) bc_first.push_back(s->coloff[col]);
+
+    s->tiled = (p.kernel == HCFD_KERNEL_TILED);
+    // tiled kernels: one compute thread per tile cell unless asked otherwise
+    if (s->tiled && !p.block) s->block = std::min(p.tile ? p.tile : 128, 256);
+    std::vector<int2> slot;
+    if (s->tiled) {
+        rc = hcfd::build_tile_plan(*mv, cf_off, cf_con, ghost, perm, s->F_BC, bc_first, p.tile ? p.tile : 128,
+                                   s->W, s->plan);
+        if (rc != HCFD_OK) return rc;
+    } else {
+        // Per-cell kernels: slot-major table {face or ~face, neighbour}, internal numbering.
+        slot.assign((size_t) s->W * Nc, make_int2(-1, -1));
+        for (int ci = 0; ci < Nc; ci++) {
+            const int u = perm[ci];
+            if (ghost[u]) continue;
+            int k = 0;
+            for (int j = cf_off[u]; j < cf_off[u + 1]; j++, k++) {
+                const int f = cf_con[j];
+                const int L = mv->fc_con[2 * f], R = mv->fc_con[2 * f + 1];
+                slot[(size_t) k * Nc + ci] = (L == u) ? make_int2(f, iperm[R]) : make_int2(~f, iperm[L]);
+            }
         }
     }
 
@@ -239,53 +361,94 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
     auto bail = [&](int code) { free_all(h); s.release(); delete h; return code; };
     const bool f32 = p.precision == HCFD_FP32;
     const size_t tsz = f32 ? sizeof(float) : sizeof(double);
-    int* d_fn = nullptr; int* d_cnoff = nullptr; int* d_cncon = nullptr; int* d_cfoff = nullptr; int* d_cfcon = nullptr;
-    double* d_nodes = nullptr; double* d_xc = nullptr;
+    if (s->tiled) {
+        rc = f32 ? setup_tiled<float>(h) : setup_tiled<double>(h);
+        if (rc) return bail(rc);
+        h->partial_len = std::max(h->grid1, h->grid2);
+    } else {
+        h->partial_len = nblk(Nc, h->block);
+    }
+    int* d_fn = nullptr; int* d_fcu = nullptr; int* d_cnoff = nullptr; int* d_cncon = nullptr;
+    int* d_cfoff = nullptr; int* d_cfcon = nullptr; int* d_efid = nullptr;
+    double* d_nodes = nullptr; double* d_xc = nullptr; double* d_ivu = nullptr;
     auto free_tmp = [&]() {
         cudaStreamSynchronize(h->stream);
-        void* t[] = {d_fn, d_cnoff, d_cncon, d_cfoff, d_cfcon, d_nodes, d_xc};
+        void* t[] = {d_fn, d_fcu, d_cnoff, d_cncon, d_cfoff, d_cfcon, d_efid, d_nodes, d_xc, d_ivu};
         for (void* q : t) if (q) cudaFree(q);
     };
-    int ncn = mv->cn_off[mv->Nc];
-    if ((rc = dalloc(&h->d_fc, 2 * (size_t) h->Nf)) || (rc = dalloc(&h->d_slot, slot.size())) ||
-        (rc = dalloc((char**) &h->d_geo, tsz * 8 * h->Nf)) || (rc = dalloc(&h->d_geo64, h->Nf)) ||
-        (rc = dalloc((char**) &h->d_iv, tsz * h->Nc)) || (rc = dalloc(&h->d_iv64, h->Nc)) ||
-        (rc = dalloc((char**) &h->d_U[0], tsz * 4 * h->Nc)) || (rc = dalloc((char**) &h->d_U[1], tsz * 4 * h->Nc)) ||
-        (rc = dalloc((char**) &h->d_phiG, tsz * 8 * h->Nc)) || (rc = dalloc(&h->d_io, 4 * (size_t) h->Nc)) ||
-        (rc = dalloc(&h->d_cp, h->Nf)) || (rc = dalloc(&h->d_dtmin, 2)) ||
-        (rc = dalloc(&h->d_partial, nblk(h->Nc, h->block))) || (rc = dalloc(&h->d_counter, 1)) ||
-        (rc = dalloc(&h->d_stats, 1)) || (rc = dalloc(&d_fn, 2 * (size_t) h->Nf)) ||
-        (rc = dalloc(&d_cnoff, h->Nc + 1)) || (rc = dalloc(&d_cncon, ncn)) || (rc = dalloc(&d_cfoff, h->Nc + 1)) ||
+    const int ncn = mv->cn_off[Nc];
+    const size_t E = h->plan.efid.size();
+    // iv is read one whole tile at a time by the tiled kernels: pad it to full tiles.
+    const size_t niv = h->tiled ? std::max((size_t) Nc, (size_t) h->plan.ntiles * h->plan.B) : (size_t) Nc;
+    if ((rc = dalloc(&h->d_fc, 2 * (size_t) Nf)) || (rc = dalloc(&h->d_perm, Nc)) ||
+        (rc = dalloc(&h->d_geo64, Nf)) || (rc = dalloc((char**) &h->d_iv, tsz * niv)) ||
+        (rc = dalloc((char**) &h->d_U[0], tsz * 4 * Nc)) || (rc = dalloc((char**) &h->d_U[1], tsz * 4 * Nc)) ||
+        (rc = dalloc((char**) &h->d_phiG, tsz * 8 * Nc)) || (rc = dalloc(&h->d_io, 4 * (size_t) Nc)) ||
+        (rc = dalloc(&h->d_cp, Nf)) || (rc = dalloc(&h->d_dtmin, 2)) || (rc = dalloc(&h->d_partial, h->partial_len)) ||
+        (rc = dalloc(&h->d_counter, 1)) || (rc = dalloc(&h->d_err, 1)) || (rc = dalloc(&h->d_stats, 1)) ||
+        (rc = dalloc(&d_fn, 2 * (size_t) Nf)) || (rc = dalloc(&d_fcu, 2 * (size_t) Nf)) ||
+        (rc = dalloc(&d_cnoff, Nc + 1)) || (rc = dalloc(&d_cncon, ncn)) || (rc = dalloc(&d_cfoff, Nc + 1)) ||
         (rc = dalloc(&d_cfcon, cf_con.size())) || (rc = dalloc(&d_nodes, 2 * (size_t) h->Nn)) ||
-        (rc = dalloc(&d_xc, 2 * (size_t) h->Nc))) {
+        (rc = dalloc(&d_xc, 2 * (size_t) Nc)) || (rc = dalloc(&d_ivu, Nc))) {
         free_tmp();
         return bail(rc);
     }
+    if (h->tiled) {
+        if ((rc = dalloc((char**) &h->d_tgeo, tsz * 8 * E)) || (rc = dalloc(&h->d_tmeta, 8 * E)) ||
+            (rc = dalloc(&h->d_foff, h->plan.foff.size())) || (rc = dalloc(&h->d_hoff, h->plan.hoff.size())) ||
+            (rc = dalloc(&h->d_halo, h->plan.halo.size())) || (rc = dalloc(&h->d_cslot, h->plan.cslot.size())) ||
+            (rc = dalloc(&d_efid, E))) {
+            free_tmp();
+            return bail(rc);
+        }
+    } else {
+        if ((rc = dalloc(&h->d_slot, slot.size())) || (f32 && (rc = dalloc((char**) &h->d_geoT, tsz * 8 * (size_t) Nf)))) {
+            free_tmp();
+            return bail(rc);
+        }
+    }
     cudaStream_t st = h->stream;
     auto up = [&](void* dst, const void* src, size_t bytes) {
-        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
     };
     cudaError_t ce = cudaSuccess;
-    if (ce == cudaSuccess) ce = up(h->d_fc, mv->fc_con, 8 * (size_t) h->Nf);
-    if (ce == cudaSuccess) ce = up(d_fn, mv->fn_con, 8 * (size_t) h->Nf);
-    if (ce == cudaSuccess) ce = up(h->d_slot, slot.data(), sizeof(int2) * slot.size());
-    if (ce == cudaSuccess) ce = up(d_cnoff, mv->cn_off, 4 * (size_t) (h->Nc + 1));
+    if (ce == cudaSuccess) ce = up(h->d_fc, fc_int.data(), 8 * (size_t) Nf);
+    if (ce == cudaSuccess) ce = up(h->d_perm, perm.data(), 4 * (size_t) Nc);
+    if (ce == cudaSuccess) ce = up(d_fcu, mv->fc_con, 8 * (size_t) Nf);
+    if (ce == cudaSuccess) ce = up(d_fn, mv->fn_con, 8 * (size_t) Nf);
+    if (ce == cudaSuccess) ce = up(d_cnoff, mv->cn_off, 4 * (size_t) (Nc + 1));
     if (ce == cudaSuccess) ce = up(d_cncon, mv->cn_con, 4 * (size_t) ncn);
     if (ce == cudaSuccess) ce = up(d_cfoff, cf_off.data(), 4 * cf_off.size());
     if (ce == cudaSuccess) ce = up(d_cfcon, cf_con.data(), 4 * cf_con.size());
     if (ce == cudaSuccess) ce = up(d_nodes, mv->nodes, 16 * (size_t) h->Nn);
+    if (h->tiled) {
+        const hcfd::TilePlan& P = h->plan;
+        if (ce == cudaSuccess) ce = up(h->d_tmeta, P.meta.data(), 2 * P.meta.size());
+        if (ce == cudaSuccess) ce = up(h->d_foff, P.foff.data(), 4 * P.foff.size());
+        if (ce == cudaSuccess) ce = up(h->d_hoff, P.hoff.data(), 4 * P.hoff.size());
+        if (ce == cudaSuccess) ce = up(h->d_halo, P.halo.data(), 4 * P.halo.size());
+        if (ce == cudaSuccess) ce = up(h->d_cslot, P.cslot.data(), 2 * P.cslot.size());
+        if (ce == cudaSuccess) ce = up(d_efid, P.efid.data(), 4 * E);
+    } else {
+        if (ce == cudaSuccess) ce = up(h->d_slot, slot.data(), sizeof(int2) * slot.size());
+    }
     if (ce == cudaSuccess) {
-        hcfd::geom_xc_kernel<<<nblk(h->Nc, 256), 256, 0, st>>>(h->Nc, d_cnoff, d_cncon, d_nodes, d_xc);
-        hcfd::geom_face_kernel<<<nblk(h->Nf, 256), 256, 0, st>>>(h->Nf, h->F_BC, d_fn, h->d_fc, d_nodes, d_xc, h->d_geo64);
-        hcfd::geom_iv_kernel<<<nblk(h->Nc, 256), 256, 0, st>>>(h->Nc, h->F_BC, d_cfoff, d_cfcon, h->d_fc, h->d_geo64, h->d_iv64);
-        if (f32) {
-            hcfd::convert_geo_kernel<float><<<nblk(h->Nf, 256), 256, 0, st>>>(h->Nf, h->d_geo64, (hcfd::FaceGeo<float>*) h->d_geo);
-            hcfd::convert_iv_kernel<float><<<nblk(h->Nc, 256), 256, 0, st>>>(h->Nc, h->d_iv64, (float*) h->d_iv);
-        } else {
-            ce = cudaMemcpyAsync(h->d_geo, h->d_geo64, sizeof(hcfd::FaceGeo<double>) * h->Nf, cudaMemcpyDeviceToDevice, st);
-            if (ce == cudaSuccess)
-                ce = cudaMemcpyAsync(h->d_iv, h->d_iv64, sizeof(double) * h->Nc, cudaMemcpyDeviceToDevice, st);
+        // Geometry in double, input numbering (src/Base/Domain.cpp:4-154).
+        hcfd::geom_xc_kernel<<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_cnoff, d_cncon, d_nodes, d_xc);
+        hcfd::geom_face_kernel<<<nblk(Nf, 256), 256, 0, st>>>(Nf, h->F_BC, d_fn, d_fcu, d_nodes, d_xc, h->d_geo64);
+        hcfd::geom_iv_kernel<<<nblk(Nc, 256), 256, 0, st>>>(Nc, h->F_BC, d_cfoff, d_cfcon, d_fcu, h->d_geo64, d_ivu);
+        // iv to the internal numbering, then to T.
+        ce = cudaMemsetAsync(h->d_iv, 0, tsz * niv, st);
+        hcfd::permute_kernel<<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_ivu, h->d_perm, d_xc);
+        if (f32) hcfd::convert_iv_kernel<float><<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_xc, (float*) h->d_iv);
+        else ce = cudaMemcpyAsync(h->d_iv, d_xc, sizeof(double) * Nc, cudaMemcpyDeviceToDevice, st);
+        if (h->tiled && E) {
+            const int nt = h->plan.ntiles;
+            if (f32) hcfd::gather_geo_kernel<float><<<nt, 128, 0, st>>>(nt, h->d_foff, d_efid, h->d_geo64, (float*) h->d_tgeo);
+            else hcfd::gather_geo_kernel<double><<<nt, 128, 0, st>>>(nt, h->d_foff, d_efid, h->d_geo64, (double*) h->d_tgeo);
         }
+        if (!h->tiled && f32)
+            hcfd::convert_geo_kernel<float><<<nblk(Nf, 256), 256, 0, st>>>(Nf, h->d_geo64, (hcfd::FaceGeo<float>*) h->d_geoT);
         if (ce == cudaSuccess) ce = cudaGetLastError();
     }
     if (ce == cudaSuccess) {
@@ -293,8 +456,11 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         ce = up(h->d_dtmin, inf2, sizeof(inf2));
     }
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned int), st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_err, 0, sizeof(unsigned int), st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_stats, 0, sizeof(hcfd::StepStats), st);
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_phiG, 0, tsz * 8 * h->Nc, st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_phiG, 0, tsz * 8 * Nc, st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_U[0], 0, tsz * 4 * Nc, st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_U[1], 0, tsz * 4 * Nc, st);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
     free_tmp();
     if (ce != cudaSuccess) return bail(fail(HCFD_ECUDA, std::string("gpu_create: ") + cudaGetErrorString(ce)));
@@ -344,6 +510,7 @@ int hcfd_gpu_initialise(hcfd_solver* s, const double* qic) {
     rc = s->fp32() ? refresh_ghosts<float>(s) : refresh_ghosts<double>(s);
     if (rc) return rc;
     CK(cudaMemsetAsync(s->d_stats, 0, sizeof(hcfd::StepStats), s->stream));
+    CK(cudaMemsetAsync(s->d_err, 0, sizeof(unsigned int), s->stream));
     const unsigned long long inf2[2] = {0x7FF0000000000000ULL, 0x7FF0000000000000ULL};
     CK(cudaMemcpyAsync(s->d_dtmin, inf2, sizeof(inf2), cudaMemcpyHostToDevice, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -387,8 +554,8 @@ int hcfd_gpu_download(hcfd_solver* s, int prims, double* const* out) {
     if (rc) return rc;
     if (!out) return fail(HCFD_EINVAL, "download: null output");
     for (int v = 0; v < 4; v++) if (!out[v]) return fail(HCFD_EINVAL, "download: null output array");
-    if (s->fp32()) hcfd::out_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<float>*) s->d_U[s->cur], s->prm.gma, prims, s->d_io);
-    else hcfd::out_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<double>*) s->d_U[s->cur], s->prm.gma, prims, s->d_io);
+    if (s->fp32()) hcfd::out_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<float>*) s->d_U[s->cur], s->d_perm, s->prm.gma, prims, s->d_io);
+    else hcfd::out_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<double>*) s->d_U[s->cur], s->d_perm, s->prm.gma, prims, s->d_io);
     CK(cudaGetLastError());
     for (int v = 0; v < 4; v++)
         CK(cudaMemcpyAsync(out[v], s->d_io + (size_t) v * s->Nc, sizeof(double) * s->Nc, cudaMemcpyDeviceToHost, s->stream));
@@ -405,8 +572,8 @@ int hcfd_gpu_upload(hcfd_solver* s, const double* const* in) {
         if (!in[v]) return fail(HCFD_EINVAL, "upload: null input array");
         CK(cudaMemcpyAsync(s->d_io + (size_t) v * s->Nc, in[v], sizeof(double) * s->Nc, cudaMemcpyHostToDevice, s->stream));
     }
-    if (s->fp32()) hcfd::in_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, s->d_io, (hcfd::Cell4<float>*) s->d_U[s->cur]);
-    else hcfd::in_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, s->d_io, (hcfd::Cell4<double>*) s->d_U[s->cur]);
+    if (s->fp32()) hcfd::in_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, s->d_io, s->d_perm, (hcfd::Cell4<float>*) s->d_U[s->cur]);
+    else hcfd::in_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, s->d_io, s->d_perm, (hcfd::Cell4<double>*) s->d_U[s->cur]);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
     s->initialised = true;
@@ -422,8 +589,8 @@ int hcfd_gpu_wall_cp(hcfd_solver* s, int colour, double rho_inf, double p_inf, d
     const double qinf = 0.5 * rho_inf * speed_inf * speed_inf;
     *n = F2 - F1;
     if (F2 == F1) return HCFD_OK;
-    if (s->fp32()) hcfd::wall_cp_kernel<float><<<nblk(F2 - F1, 256), 256, 0, s->stream>>>(F1, F2, s->d_fc, (const hcfd::Cell4<float>*) s->d_U[s->cur], s->prm.gma, p_inf, qinf, s->d_cp);
-    else hcfd::wall_cp_kernel<double><<<nblk(F2 - F1, 256), 256, 0, s->stream>>>(F1, F2, s->d_fc, (const hcfd::Cell4<double>*) s->d_U[s->cur], s->prm.gma, p_inf, qinf, s->d_cp);
+    if (s->fp32()) hcfd::wall_cp_kernel<float><<<nblk(F2 - F1, 256), 256, 0, s->stream>>>(s->Nc, F1, F2, s->d_fc, (const hcfd::Cell4<float>*) s->d_U[s->cur], s->prm.gma, p_inf, qinf, s->d_cp);
+    else hcfd::wall_cp_kernel<double><<<nblk(F2 - F1, 256), 256, 0, s->stream>>>(s->Nc, F1, F2, s->d_fc, (const hcfd::Cell4<double>*) s->d_U[s->cur], s->prm.gma, p_inf, qinf, s->d_cp);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, s->d_cp, sizeof(double) * (F2 - F1), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));

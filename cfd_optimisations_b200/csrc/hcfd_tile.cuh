@@ -1,0 +1,569 @@
+// Tiled step kernels: persistent CTAs walk the tiles of the execution plan (hcfd_plan.cpp).
+// Per tile, the contiguous blocks (the tile's own cells, its face records and face
+// metadata) are staged into shared memory with TMA bulk copies (cp.async.bulk, completion
+// on an mbarrier) and the halo cells with 16-byte cp.async gathers; all arithmetic then
+// reads shared memory.
+//
+// pass 1 (thread per tile cell): Green-Gauss gradient, limiter, CFL dt -> phiG (global).
+// pass 2: face phase (thread per face entry) computes each face flux once per tile and
+//         writes (A_f, F) into the flux slot of each tile cell the face borders; cell phase
+//         (thread per tile cell) sums its slots in increasing face order, updates the cell
+//         and refreshes its ghost cells.
+// The arithmetic is that of the thread-per-cell kernels in hcfd_kernels.cuh, operation for
+// operation; only where the operands come from differs.
+#pragma once
+#include "hcfd_kernels.cuh"
+
+namespace hcfd {
+
+template <class T>
+struct TileArgs {
+    StepArgs<T> s;                         // state, stats, BC table, modes
+    const T* __restrict__ tgeo;            // face records, per tile component-major: [8][nf]
+    const short* __restrict__ tmeta;       // 8 shorts per entry: la, lb, slotL, slotR, bc, 0, 0, 0
+    const int* __restrict__ foff;          // [ntiles + 1], multiples of 4
+    const int* __restrict__ hoff;          // [ntiles + 1]
+    const int* __restrict__ halo;          // internal cell ids
+    const short* __restrict__ cslot;       // [ntiles * B * Wp]: (entry << 1) | cell-is-right, or -1
+    int ntiles, B, Wp, Hmax, Fmax;
+    unsigned int* err;                     // bit 0: a bounded wait gave up
+};
+
+// ---------------------------------------------------------------------------------------
+// PTX helpers (sm_90+ bulk copies and mbarriers; sm_80+ cp.async)
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// 1-D bulk copy global -> shared (no tensor map, no multicast); dst, src 16-B aligned,
+// bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Bounded wait for an mbarrier phase: gives up after ~2^22 polls, records the failure and
+// returns false (the kernel then finishes its tile loop with whatever data it has; the
+// host reports HCFD_ETIMEOUT).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned int* err) {
+#pragma unroll 1
+    for (int i = 0; i < (1 << 22); i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicOr(err, 1u);
+    return false;
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Shared-memory loads (plain loads: the __ldg helpers of hcfd_kernels.cuh are global-only).
+// (chunk-plane layout of hcfd_kernels.cuh, plane stride ps = staged cell count)
+__device__ __forceinline__ void lds_cell(const Cell4<double>* p, int ps, int i, double u[4]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = q[i], b = q[ps + i];
+    u[0] = a.x; u[1] = a.y; u[2] = b.x; u[3] = b.y;
+}
+__device__ __forceinline__ void lds_cell(const Cell4<float>* p, int, int i, float u[4]) {
+    const float4 a = reinterpret_cast<const float4*>(p)[i];
+    u[0] = a.x; u[1] = a.y; u[2] = a.z; u[3] = a.w;
+}
+__device__ __forceinline__ void lds_grad(const Grad8<double>* p, int ps, int i, double g[8]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int k = 0; k < 4; k++) { const double2 a = q[k * ps + i]; g[2 * k] = a.x; g[2 * k + 1] = a.y; }
+}
+__device__ __forceinline__ void lds_grad(const Grad8<float>* p, int ps, int i, float g[8]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 a = q[i], b = q[ps + i];
+    g[0] = a.x; g[1] = a.y; g[2] = a.z; g[3] = a.w; g[4] = b.x; g[5] = b.y; g[6] = b.z; g[7] = b.w;
+}
+// Face record e of a tile whose records are stored component-major ([8][nf]): consecutive
+// threads reading consecutive records touch consecutive words (no bank conflicts).
+template <class T>
+__device__ __forceinline__ void lds_geo(const T* p, int nf, int e, FaceGeo<T>& g) {
+    g.nx = p[e]; g.ny = p[nf + e]; g.Af = p[2 * nf + e]; g.If = p[3 * nf + e];
+    g.rLx = p[4 * nf + e]; g.rLy = p[5 * nf + e]; g.rRx = p[6 * nf + e]; g.rRy = p[7 * nf + e];
+}
+
+__host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~size_t(127); }
+
+// Shared-memory layout of one CTA: two mbarriers, two staging buffers (double buffering:
+// tile i+1 is in flight while tile i is computed) and, for pass 2, one flux-slot scratch.
+// One staging buffer holds the tile's and its halo's cells (and limited gradients in
+// pass 2), its face records and metadata, its slot table and its iv.
+template <class T>
+struct TileSmem {
+    size_t u, g, geo, meta, cslot, iv, stage, flux, total;   // byte offsets within a stage
+    __host__ __device__ TileSmem(int B, int Hmax, int Fmax, int W, int Wp, bool pass2) {
+        size_t p = 0;
+        u = p;     p += align128((size_t) (B + Hmax) * sizeof(Cell4<T>));
+        g = p;     if (pass2) p += align128((size_t) (B + Hmax) * sizeof(Grad8<T>));
+        geo = p;   p += align128((size_t) Fmax * sizeof(FaceGeo<T>));
+        meta = p;  p += align128((size_t) Fmax * 16);
+        cslot = p; p += align128((size_t) B * Wp * sizeof(short));
+        iv = p;    p += align128((size_t) B * sizeof(T));
+        stage = p;
+        flux = 128 + 2 * stage;
+        total = flux + (pass2 ? align128((size_t) 5 * B * W * sizeof(T)) : 0);
+    }
+};
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Arrival on `bar` once all cp.async operations issued so far by this thread have landed;
+// counts as one of the barrier's expected arrivals (.noinc).
+__device__ __forceinline__ void cp_async_arrive_noinc(unsigned long long* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Barrier over the compute warps only (named barrier 1; the producer warp never joins it).
+__device__ __forceinline__ void compute_sync(int nthreads) {
+    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+// Producer warp: for each of this CTA's tiles, waits until the compute warps have released
+// the staging buffer, then lane 0 arms the buffer's `full` mbarrier with the byte count of
+// the bulk copies and issues them, and every lane gathers its share of the halo cells with
+// cp.async and signals their completion on the same mbarrier.  The `full` barrier therefore
+// completes when all of the tile's data has landed: 1 expect-tx arrival + 32 cp.async
+// arrivals + the transaction bytes.
+template <class T, bool PASS2>
+__device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned char* smem, unsigned long long* full,
+                                              unsigned long long* empty, const TileSmem<T>& L) {
+    const int lane = threadIdx.x & 31;
+    constexpr int CU = sizeof(Cell4<T>) / 16, CG = PASS2 ? sizeof(Grad8<T>) / 16 : 0;
+    const int NL = a.B + a.Hmax;   // plane stride of the staged cells
+    unsigned iter = 0;
+    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {
+        const int buf = iter & 1;
+        if (iter >= 2) mbar_wait(empty + buf, ((iter >> 1) - 1) & 1, a.err);
+        unsigned char* st = smem + 128 + buf * L.stage;
+        const int base = t * a.B, nb = min(a.B, a.s.Nc - base);
+        const int f0 = __ldg(a.foff + t), nf = __ldg(a.foff + t + 1) - f0;
+        const int h0 = __ldg(a.hoff + t), nh = __ldg(a.hoff + t + 1) - h0;
+        Cell4<T>* sU = reinterpret_cast<Cell4<T>*>(st + L.u);
+        Grad8<T>* sG = reinterpret_cast<Grad8<T>*>(st + L.g);
+        if (lane == 0) {
+            const unsigned bu = nb * sizeof(Cell4<T>), bg = PASS2 ? nb * sizeof(Grad8<T>) : 0u;
+            const unsigned bf = nf * sizeof(FaceGeo<T>), bm = nf * 16u;
+            const unsigned bs = a.B * a.Wp * sizeof(short), bi = a.B * sizeof(T);
+            // the tile's entry count, for the consumers' component-major indexing; published
+            // by the release of the arrive below
+            reinterpret_cast<int*>(smem + 64)[buf] = nf;
+            mbar_arrive_expect_tx(full + buf, bu + bg + bf + bm + bs + bi);
+            // one bulk copy per 16-byte chunk plane of the tile's cell range
+#pragma unroll
+            for (int j = 0; j < CU; j++)
+                bulk_g2s(reinterpret_cast<char*>(sU) + (size_t) 16 * j * NL,
+                         reinterpret_cast<const char*>(a.s.U) + 16 * ((size_t) j * a.s.Nc + base), nb * 16u, full + buf);
+            if (PASS2) {
+#pragma unroll
+                for (int j = 0; j < CG; j++)
+                    bulk_g2s(reinterpret_cast<char*>(sG) + (size_t) 16 * j * NL,
+                             reinterpret_cast<const char*>(a.s.phiG) + 16 * ((size_t) j * a.s.Nc + base), nb * 16u,
+                             full + buf);
+            }
+            if (bf) {
+                bulk_g2s(st + L.geo, a.tgeo + (size_t) f0 * 8, bf, full + buf);
+                bulk_g2s(st + L.meta, a.tmeta + (size_t) f0 * 8, bm, full + buf);
+            }
+            bulk_g2s(st + L.cslot, a.cslot + (size_t) t * a.B * a.Wp, bs, full + buf);
+            bulk_g2s(st + L.iv, a.s.iv + base, bi, full + buf);
+        }
+        for (int h = lane; h < nh; h += 32) {
+            const int ci = __ldg(a.halo + h0 + h);
+#pragma unroll
+            for (int j = 0; j < CU; j++)
+                cp_async16(reinterpret_cast<char*>(sU) + 16 * ((size_t) j * NL + a.B + h),
+                           reinterpret_cast<const char*>(a.s.U) + 16 * ((size_t) j * a.s.Nc + ci));
+#pragma unroll
+            for (int j = 0; j < CG; j++)
+                cp_async16(reinterpret_cast<char*>(sG) + 16 * ((size_t) j * NL + a.B + h),
+                           reinterpret_cast<const char*>(a.s.phiG) + 16 * ((size_t) j * a.s.Nc + ci));
+        }
+        cp_async_arrive_noinc(full + buf);
+    }
+}
+
+// Residual / non-finite / dt bookkeeping shared by the last pass of a step.
+template <class T>
+__device__ __forceinline__ void finish_step(const StepArgs<T>& a, double r2, int bad, double dt_used) {
+    __shared__ double sm[32];
+    __shared__ int smbad[32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double w = warp_sum(r2);
+    int wb = __any_sync(0xffffffffu, bad);
+    if (lane == 0) { sm[wid] = w; smbad[wid] = wb; }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (int) (blockDim.x >> 5);
+        double x = lane < nw ? sm[lane] : 0.0;
+        int xb = lane < nw ? smbad[lane] : 0;
+        x = warp_sum(x);
+        xb = __any_sync(0xffffffffu, xb);
+        if (lane == 0) {
+            a.partial[blockIdx.x] = x;
+            if (xb) atomicOr(&a.stats->nonfinite, 1);
+            __threadfence();
+            const unsigned int done = atomicAdd(a.counter, 1u);
+            last = (done == gridDim.x - 1);
+        }
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double x = 0.0;
+        for (int i = threadIdx.x; i < (int) gridDim.x; i += blockDim.x) x += ((volatile double*) a.partial)[i];
+        x = warp_sum(x);
+        if (lane == 0) sm[wid] = x;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int i = 0; i < (int) (blockDim.x >> 5); i++) tot += sm[i];
+            StepStats* st = a.stats;
+            st->res2_last = tot;
+            if (st->steps == 0) st->res2_first = tot;
+            st->steps += 1;
+            st->dt_last = dt_used;
+            if (!(tot == tot) || tot > 1.7e308) st->nonfinite = 1;
+            *a.counter = 0u;
+            if (a.time_mode != TM_FIXED) *a.dtmin_next = 0x7FF0000000000000ULL;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+
+__device__ __forceinline__ void lds_slots(const short* p, int Wp, short cs[8]) {
+    if (Wp == 4) {
+        const short4 a = *reinterpret_cast<const short4*>(p);
+        cs[0] = a.x; cs[1] = a.y; cs[2] = a.z; cs[3] = a.w;
+        cs[4] = cs[5] = cs[6] = cs[7] = -1;
+    } else {
+        const int4 a = *reinterpret_cast<const int4*>(p);
+        const short* q = reinterpret_cast<const short*>(&a);
+#pragma unroll
+        for (int k = 0; k < 8; k++) cs[k] = q[k];
+    }
+}
+
+// One face entry of pass 2: operands gathered from shared memory and reduced at once to the
+// MUSCL states on both sides (Flux.cpp:83-87), then the Rusanov flux in the face's own
+// L -> R orientation.  Only the reconstructed states stay live between load and flux.
+template <class T>
+struct FaceIn {
+    T uoL[4], uqR[4], nx, ny, Af;
+    int sL, sR;
+    __device__ __forceinline__ void load(const Cell4<T>* sU, const Grad8<T>* sG, int NL, const T* sGeo,
+                                         const short* sMeta, int nf, int e) {
+        const short4 m = *reinterpret_cast<const short4*>(sMeta + 8 * e);
+        sL = m.z; sR = m.w;
+        const int bc = sMeta[8 * e + 4];
+        FaceGeo<T> g;
+        lds_geo(sGeo, nf, e, g);
+        nx = g.nx; ny = g.ny; Af = g.Af;
+        T uL[4], uR[4], gL[8];
+        lds_cell(sU, NL, m.x, uL);
+        lds_cell(sU, NL, m.y, uR);
+        lds_grad(sG, NL, m.x, gL);
+        if (bc >= 0) {
+            // Ghost on the right: -grad and the same phi as the interior cell with r_R = -r_L
+            // (BoundaryConditions/Base.cpp:29-53, Domain.cpp:84-88): the same increment.
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                const T du = gL[2 * v] * g.rLx + gL[2 * v + 1] * g.rLy;
+                uoL[v] = uL[v] + du;
+                uqR[v] = uR[v] + du;
+            }
+        } else {
+            T gR[8];
+            lds_grad(sG, NL, m.y, gR);
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                uoL[v] = uL[v] + (gL[2 * v] * g.rLx + gL[2 * v + 1] * g.rLy);
+                uqR[v] = uR[v] + (gR[2 * v] * g.rRx + gR[2 * v + 1] * g.rRy);
+            }
+        }
+    }
+    __device__ __forceinline__ void flux(T gma, T F[4]) const { rusanov(uoL, uqR, nx, ny, gma, F); }
+    __device__ __forceinline__ void store(T* sF, int BW, const T F[4]) const {
+        if (sL >= 0) {
+            sF[sL] = Af;
+#pragma unroll
+            for (int v = 0; v < 4; v++) sF[(v + 1) * BW + sL] = F[v];
+        }
+        if (sR >= 0) {
+            sF[sR] = Af;
+#pragma unroll
+            for (int v = 0; v < 4; v++) sF[(v + 1) * BW + sR] = F[v];
+        }
+    }
+};
+
+// Warp-specialised persistent tile loop.  The last warp of the CTA is the producer
+// (producer_loop); the first NT = blockDim.x - 32 threads compute.  Compute iteration i
+// reads staging buffer i & 1 once its `full` barrier completes and releases it on its
+// `empty` barrier (one arrival per compute warp) when done.
+#define HCFD_TILE_LOOP_BEGIN(PASS2)                                                              \
+    const int NT = blockDim.x - 32;                                                              \
+    const int NL = a.B + a.Hmax;                                                                 \
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(smem);                      \
+    unsigned long long* empty = full + 2;                                                        \
+    if (threadIdx.x == 0) {                                                                      \
+        mbar_init(full, 33); mbar_init(full + 1, 33);                                            \
+        mbar_init(empty, NT / 32); mbar_init(empty + 1, NT / 32);                                \
+        fence_mbar_init();                                                                       \
+    }                                                                                            \
+    __syncthreads();                                                                             \
+    if ((int) threadIdx.x >= NT) {                                                               \
+        producer_loop<T, PASS2>(a, smem, full, empty, L);                                        \
+    } else {                                                                                     \
+    unsigned iter = 0;                                                                           \
+    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {                             \
+        const int buf = iter & 1;                                                                \
+        unsigned char* st = smem + 128 + buf * L.stage;                                          \
+        mbar_wait(full + buf, (iter >> 1) & 1, a.err);                                           \
+        const int base = t * a.B, nb = min(a.B, s.Nc - base);                                    \
+        const Cell4<T>* sU = reinterpret_cast<const Cell4<T>*>(st + L.u);                        \
+        const T* sGeo = reinterpret_cast<const T*>(st + L.geo);                                  \
+        const int nfl = reinterpret_cast<const int*>(smem + 64)[buf];                            \
+        const short* sMeta = reinterpret_cast<const short*>(st + L.meta);                        \
+        const short* sSlot = reinterpret_cast<const short*>(st + L.cslot);                       \
+        const T* sIv = reinterpret_cast<const T*>(st + L.iv);
+
+#define HCFD_TILE_LOOP_END                                                                       \
+        __syncwarp();                                                                            \
+        if ((threadIdx.x & 31) == 0) mbar_arrive(empty + buf);                                   \
+    }                                                                                            \
+    }
+
+template <class T, int W>
+__global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const TileSmem<T> L(a.B, a.Hmax, a.Fmax, W, a.Wp, false);
+    const StepArgs<T>& s = a.s;
+    double dtc = 1e300;
+    HCFD_TILE_LOOP_BEGIN(false)
+    for (int c = threadIdx.x; c < nb; c += NT) {
+        short cs[8];
+        lds_slots(sSlot + c * a.Wp, a.Wp, cs);
+        if (cs[0] < 0) continue;
+        T u[4];
+        lds_cell(sU, NL, c, u);
+        const T iv = sIv[c];
+        T G[4][2], umin[4], umax[4], ro[W][2];
+#pragma unroll
+        for (int v = 0; v < 4; v++) { G[v][0] = T(0); G[v][1] = T(0); umin[v] = u[v]; umax[v] = u[v]; }
+        T cu = T(0), cv = T(0), ca = T(0), lam = T(0);
+        if (s.time_mode != TM_FIXED) cell_speed(u, s.gma, cu, cv, ca);
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+            ro[k][0] = T(0); ro[k][1] = T(0);
+            if (cs[k] < 0) continue;
+            const int e = cs[k] >> 1;
+            const bool isL = (cs[k] & 1) == 0;
+            FaceGeo<T> g;
+            lds_geo(sGeo, nfl, e, g);
+            const int nbl = isL ? sMeta[8 * e + 1] : sMeta[8 * e];
+            T un[4];
+            lds_cell(sU, NL, nbl, un);
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                // GaussGreen.cpp:25-28 and Limiter.cpp:31-39
+                const T uL = isL ? u[v] : un[v];
+                const T uR = isL ? un[v] : u[v];
+                const T uf = uL * g.If + uR * (T(1) - g.If);
+                const T tt = uf * g.Af;
+                if (isL) { G[v][0] += tt * g.nx; G[v][1] += tt * g.ny; }
+                else     { G[v][0] -= tt * g.nx; G[v][1] -= tt * g.ny; }
+                umin[v] = fmin(umin[v], un[v]);
+                umax[v] = fmax(umax[v], un[v]);
+            }
+            ro[k][0] = isL ? g.rLx : g.rRx;
+            ro[k][1] = isL ? g.rLy : g.rRy;
+            if (s.time_mode != TM_FIXED) lam += wave(cu, cv, ca, g);
+        }
+        T e2 = T(0);
+        if (s.limiter == LIM_VENKAT) {
+            const T kh = s.venkat_K * sqrt(T(1) / iv);
+            e2 = kh * kh * kh;
+        }
+        const T eps = T(1e-9);
+        T out[8];
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const T gx = G[v][0] * iv, gy = G[v][1] * iv;
+            T phi = T(1);
+#pragma unroll
+            for (int k = 0; k < W; k++) {
+                if (cs[k] < 0) continue;
+                const T d = gx * ro[k][0] + gy * ro[k][1];
+                T pf = T(1);
+                if (s.limiter == LIM_BJ) {                       // Limiter.cpp:67-71
+                    // one division: the numerator is picked by the sign of d
+                    if (d > eps || d < -eps) pf = fmin(T(1), ((d > eps) ? umax[v] - u[v] : umin[v] - u[v]) / d);
+                } else {
+                    if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
+                }
+                phi = fmin(phi, pf);
+            }
+            out[2 * v] = phi * gx;
+            out[2 * v + 1] = phi * gy;
+        }
+        st_grad(s.phiG, s.Nc, base + c, out);
+        if (s.time_mode != TM_FIXED) dtc = fmin(dtc, (double) (T(1) / (iv * lam)));
+    }
+    HCFD_TILE_LOOP_END
+    if (s.time_mode != TM_FIXED) {
+        __shared__ double sm[32];
+        double m = warp_min(dtc);
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) sm[wid] = m;
+        __syncthreads();
+        if (wid == 0) {
+            m = lane < (int) (blockDim.x >> 5) ? sm[lane] : 1e300;
+            m = warp_min(m);
+            if (lane == 0 && m < 1e300) atomicMin(s.dtmin, (unsigned long long) __double_as_longlong(m));
+        }
+    }
+}
+
+template <class T, int W, bool COMP>
+__global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const TileSmem<T> L(a.B, a.Hmax, a.Fmax, W, a.Wp, true);
+    const StepArgs<T>& s = a.s;
+    T* sF = reinterpret_cast<T*>(smem + L.flux);     // [5][B * W]: Af, F0..F3
+    const int BW = a.B * W;
+    const double dt_used = (s.time_mode == TM_FIXED) ? s.dt_or_cfl
+                                                      : s.dt_or_cfl * __longlong_as_double((long long) *s.dtmin);
+    double r2 = 0.0;
+    int bad = 0;
+    HCFD_TILE_LOOP_BEGIN(true)
+    const Grad8<T>* sG = reinterpret_cast<const Grad8<T>*>(st + L.g);
+    const int nf = nfl;
+    // face phase: one Rusanov flux per face entry (Flux.cpp:19-38).  Each thread takes two
+    // entries per round and computes both before storing either, so the two independent
+    // FP64 dependency chains (divisions, square roots) interleave.
+    for (int e = threadIdx.x; e < nf; e += 2 * NT) {
+        const int eB = (e + NT < nf) ? e + NT : e;
+        FaceIn<T> A, Bq;
+        A.load(sU, sG, NL, sGeo, sMeta, nf, e);
+        Bq.load(sU, sG, NL, sGeo, sMeta, nf, eB);
+        T FA[4], FB[4];
+        A.flux(s.gma, FA);
+        Bq.flux(s.gma, FB);
+        A.store(sF, BW, FA);
+        if (eB != e) Bq.store(sF, BW, FB);
+    }
+    compute_sync(NT);
+    // cell phase: slots in increasing face order, update, ghost refresh
+    for (int c = threadIdx.x; c < nb; c += NT) {
+        short cs[8];
+        lds_slots(sSlot + c * a.Wp, a.Wp, cs);
+        if (cs[0] < 0) continue;
+        T u[4];
+        lds_cell(sU, NL, c, u);
+        const T iv = sIv[c];
+        T R[4], Rc[4];
+#pragma unroll
+        for (int v = 0; v < 4; v++) { R[v] = T(0); Rc[v] = T(0); }
+        T cu = T(0), cv = T(0), ca = T(0), lam = T(0);
+        if (s.time_mode == TM_LOCAL) cell_speed(u, s.gma, cu, cv, ca);
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+            if (cs[k] < 0) continue;
+            const bool isL = (cs[k] & 1) == 0;
+            const int sl = c * W + k;
+            const T Af = sF[sl];
+#pragma unroll
+            for (int v = 0; v < 4; v++) {                        // Flux.cpp:39-42
+                const T Fv = sF[(v + 1) * BW + sl];
+                if constexpr (COMP) {
+                    const T x = isL ? -(Af * Fv) : Af * Fv;
+                    two_sum(R[v], Rc[v], x);
+                } else {
+                    if (isL) R[v] -= Af * Fv;
+                    else     R[v] += Af * Fv;
+                }
+            }
+            if (s.time_mode == TM_LOCAL) {
+                FaceGeo<T> g;
+                lds_geo(sGeo, nfl, cs[k] >> 1, g);
+                lam += wave(cu, cv, ca, g);
+            }
+        }
+        T dt;
+        if (s.time_mode == TM_LOCAL) dt = T(s.dt_or_cfl) * (T(1) / (iv * lam));
+        else dt = T(dt_used);
+        T un_[4];
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            T Rv = COMP ? R[v] + Rc[v] : R[v];
+            Rv = Rv * iv;                                        // Flux.cpp:45-49
+            un_[v] = u[v] + dt * Rv;                             // Euler.cpp:107-113
+            if (v == 0) r2 += (double) Rv * (double) Rv;
+            bad |= !isfinite(un_[v]);
+        }
+        st_cell(s.Unew, s.Nc, base + c, un_);
+        // ghost refresh (Euler.cpp:96, :138-142): this cell is its ghosts' only neighbour
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+            if (cs[k] < 0 || (cs[k] & 1)) continue;
+            const int e = cs[k] >> 1;
+            const int bc = sMeta[8 * e + 4];
+            if (bc < 0) continue;
+            const int lb = sMeta[8 * e + 1];
+            const int gi = lb < a.B ? base + lb : __ldg(a.halo + a.hoff[t] + lb - a.B);
+            FaceGeo<T> g;
+            lds_geo(sGeo, nfl, e, g);
+            T ug[4];
+            ghost_state(s.bc.type[bc], un_, g.nx, g.ny, s.gma, s.bc.UBC[bc], s.bc.QBC[bc], ug);
+            st_cell(s.Unew, s.Nc, gi, ug);
+        }
+    }
+    compute_sync(NT);   // the next tile's face phase overwrites the flux slots
+    HCFD_TILE_LOOP_END
+    finish_step(s, r2, bad, dt_used);
+}
+
+// Face records in tile order, component-major per tile: for tile t with entries
+// [f0, f0 + nf), component k of entry e is tgeo[8 f0 + k nf + e] (zeros for padding).
+template <class T>
+__global__ void gather_geo_kernel(int ntiles, const int* __restrict__ foff, const int* __restrict__ efid,
+                                  const FaceGeo<double>* __restrict__ geo, T* __restrict__ tgeo) {
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const int f0 = foff[t], nf = foff[t + 1] - f0;
+    T* out = tgeo + (size_t) 8 * f0;
+    for (int e = threadIdx.x; e < nf; e += blockDim.x) {
+        const int f = efid[f0 + e];
+        double c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (f >= 0) {
+            const FaceGeo<double> g = geo[f];
+            c[0] = g.nx; c[1] = g.ny; c[2] = g.Af; c[3] = g.If; c[4] = g.rLx; c[5] = g.rLy; c[6] = g.rRx; c[7] = g.rRy;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) out[k * nf + e] = T(c[k]);
+    }
+}
+
+}  // namespace hcfd

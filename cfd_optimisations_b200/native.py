@@ -18,6 +18,7 @@ LIMITER_BJ, LIMITER_VENKAT = 0, 1
 FIXED_DT, GLOBAL_CFL, LOCAL_CFL = 0, 1, 2
 FP64, FP32 = 0, 1
 NUMBER_NATURAL, NUMBER_RANDOM, NUMBER_RCM, NUMBER_MORTON = 0, 1, 2, 3
+KERNEL_TILED, KERNEL_CELL = 0, 1
 
 _dp = ct.POINTER(ct.c_double)
 _ip = ct.POINTER(ct.c_int)
@@ -38,7 +39,8 @@ class WedgeSpec(ct.Structure):
 
 class Params(ct.Structure):
     _fields_ = [("gma", ct.c_double), ("limiter", ct.c_int), ("venkat_K", ct.c_double),
-                ("precision", ct.c_int), ("block", ct.c_int)]
+                ("precision", ct.c_int), ("block", ct.c_int), ("kernel", ct.c_int), ("tile", ct.c_int),
+                ("keep_numbering", ct.c_int)]
 
 
 class StepStats(ct.Structure):
@@ -82,6 +84,7 @@ _SIGS = {
     "hcfd_host_pin": (ct.c_int, [ct.c_void_p, ct.c_size_t]),
     "hcfd_host_unpin": (ct.c_int, [ct.c_void_p]),
     "hcfd_write_hsln": (ct.c_int, [ct.c_char_p, ct.c_int, ct.POINTER(ct.c_char_p), ct.c_int, ct.POINTER(_dp)]),
+    "hcfd_plan_check": (ct.c_int, [ct.POINTER(MeshView), ct.c_int, ct.c_int, ct.POINTER(ct.c_longlong)]),
     "hcfd_set_device": (ct.c_int, [ct.c_int, _ip]),
     "hcfd_device_sync": (ct.c_int, []),
     "hcfd_last_error": (ct.c_char_p, []),

@@ -130,8 +130,19 @@ typedef struct hcfd_params {
     int    limiter;     /* enum hcfd_limiter                                                 */
     double venkat_K;    /* Venkatakrishnan constant (limiter == HCFD_LIMITER_VENKAT)         */
     int    precision;   /* enum hcfd_precision                                               */
-    int    block;       /* threads per block of the step kernels, 0 = default               */
+    int    block;       /* compute threads per block of the step kernels (multiple of 32; at
+                           most 256 for the tiled kernels), 0 = 256 for the per-cell kernels
+                           and one thread per tile cell for the tiled kernels               */
+    int    kernel;      /* enum hcfd_kernel                                                  */
+    int    tile;        /* cells per tile of the tiled kernels (32..512, multiple of 32), 0 = 128 */
+    int    keep_numbering; /* 1: keep the input cell order on the device instead of the Morton order */
 } hcfd_params;
+
+/* Step kernels.  HCFD_KERNEL_TILED (default): persistent CTAs stage tiles of cells, their
+ * faces and their halo in shared memory (TMA bulk copies) and compute each face flux once
+ * per tile.  HCFD_KERNEL_CELL: one thread per cell gathering its faces from global memory.
+ * Both form every per-cell sum in the same order and give the same results. */
+enum hcfd_kernel { HCFD_KERNEL_TILED = 0, HCFD_KERNEL_CELL = 1 };
 
 typedef struct hcfd_step_stats {
     double dt;          /* dt of the last step (minimum local dt under HCFD_LOCAL_CFL)       */
@@ -196,6 +207,14 @@ void hcfd_gpu_destroy(hcfd_solver* s);
  * hcfd_gpu_download from and to it run as direct DMA; hcfd_host_unpin releases it. */
 int  hcfd_host_pin(void* p, size_t bytes);
 int  hcfd_host_unpin(void* p);
+
+/* Builds the tiled kernels' execution plan for a mesh on the host (no device needed) and
+ * checks every index the kernels derive from it: local cell indices inside the staged
+ * range, each flux slot written by exactly one face entry, slots in increasing face order,
+ * bulk-copy sizes and offsets multiples of 16 bytes.  info (8 values, may be NULL): tiles,
+ * max halo, max face entries, entries, faces computed once (both cells in one tile), cut
+ * face entries, slots per cell, total halo cells.  No reference counterpart. */
+int  hcfd_plan_check(const hcfd_mesh_view* mesh, int tile, int keep_numbering, long long* info);
 
 /* ---- output ------------------------------------------------------------------------- */
 

@@ -50,20 +50,22 @@ def test_initial_state_matches_base0(golden):
     assert np.all(O.rel_linf(s.Q(), b0) <= 1e-15)
 
 
-def test_one_step_matches_oracle_wedge(golden):
+@pytest.mark.parametrize("kernel", [H.KERNEL_TILED, H.KERNEL_CELL])
+def test_one_step_matches_oracle_wedge(golden, kernel):
     m = H.Mesh(os.path.join(golden, "wedge.hmsh"))
     case = wedge_reference_case()
-    s = solver_for(m, *case)
+    s = solver_for(m, *case, kernel=kernel)
     o = oracle_for(m, *case)
     s.step(1, H.FIXED_DT, 1e-3)
     o.step(O.FIXED_DT, 1e-3)
     assert np.all(O.rel_linf(s.U(), o.U()) <= ONE_STEP)
 
 
-def test_1000_steps_match_base1(golden):
+@pytest.mark.parametrize("kernel", [H.KERNEL_TILED, H.KERNEL_CELL])
+def test_1000_steps_match_base1(golden, kernel):
     """The reference's shipped golden: wedge.hmsh, 1000 steps of dt = 1e-3."""
     m = H.Mesh(os.path.join(golden, "wedge.hmsh"))
-    s = solver_for(m, *wedge_reference_case())
+    s = solver_for(m, *wedge_reference_case(), kernel=kernel)
     s.step(1000, H.FIXED_DT, 1e-3)
     _, b1 = O.read_hsln(os.path.join(golden, "Base_1.hsln"))
     assert np.all(O.rel_linf(s.Q(), b1) <= MANY_STEPS)
@@ -90,14 +92,15 @@ def test_generated_wedge_matches_reference_fixture(golden):
     assert np.all(O.rel_linf(s2.U(), ref["U_cfl20"]) <= 1e-11)
 
 
+@pytest.mark.parametrize("kernel", [H.KERNEL_TILED, H.KERNEL_CELL])
 @pytest.mark.parametrize("numbering", [H.NUMBER_RANDOM, H.NUMBER_RCM])
 @pytest.mark.parametrize("limiter,K", [(H.LIMITER_BJ, 0.0), (H.LIMITER_VENKAT, 5.0)])
 @pytest.mark.parametrize("mode", [H.GLOBAL_CFL, H.LOCAL_CFL])
-def test_cfl_modes_and_limiters_match_oracle(numbering, limiter, K, mode):
+def test_cfl_modes_and_limiters_match_oracle(numbering, limiter, K, mode, kernel):
     """The configuration of the 161 x 81 wedge (M = 2.5, 15 deg), 20 steps at CFL 0.5."""
     m = H.Mesh.wedge(161, 81, theta_deg=15.0, seed=1234, numbering=numbering)
     case = H.wedge_case(2.5)
-    s = solver_for(m, *case, limiter=limiter, venkat_K=K)
+    s = solver_for(m, *case, limiter=limiter, venkat_K=K, kernel=kernel)
     o = oracle_for(m, *case, limiter=limiter, K=K)
     for i in range(20):
         st = s.step(1, mode, 0.5)
@@ -179,3 +182,23 @@ def test_upload_download_roundtrip():
     U = s.U() * 1.01
     s.upload(U)
     assert np.array_equal(s.U(), U)
+
+
+@pytest.mark.parametrize("precision", [H.FP64, H.FP32])
+@pytest.mark.parametrize("tile", [0, 64])
+def test_kernel_families_and_orders_agree(precision, tile):
+    """Tiled vs per-cell kernels, Morton vs input order: every per-cell sum is formed in the
+    same order, so the states agree to rounding of the fused multiply-adds the compiler picks
+    in each kernel (bit-identical when it picks the same)."""
+    m = H.Mesh.wedge(161, 81, seed=21, numbering=H.NUMBER_RANDOM)
+    case = H.wedge_case(2.5)
+    runs = []
+    for kw in (dict(kernel=H.KERNEL_TILED, tile=tile), dict(kernel=H.KERNEL_CELL),
+               dict(kernel=H.KERNEL_TILED, tile=tile, keep_numbering=True),
+               dict(kernel=H.KERNEL_CELL, keep_numbering=True)):
+        s = solver_for(m, *case, limiter=H.LIMITER_VENKAT, venkat_K=5.0, precision=precision, **kw)
+        s.step(40, H.GLOBAL_CFL, 0.5)
+        runs.append(s.U())
+    tol = 1e-13 if precision == H.FP64 else 1e-6
+    for r in runs[1:]:
+        assert np.all(O.rel_linf(r, runs[0]) <= tol)
