@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(256) pass2_kernel(const StepArgs<T> a) {
 // geometry precompute (double), src/Base/Domain.cpp:44-154
 
 // Domain::compute_xc (:61-71): vertex average, summed node by node in cn_con order.
-__global__ void geom_xc_kernel(int Nc, const int* __restrict__ cn_off, const int* __restrict__ cn_con,
+static __global__ void geom_xc_kernel(int Nc, const int* __restrict__ cn_off, const int* __restrict__ cn_con,
                                const double* __restrict__ nodes, double* __restrict__ xc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= Nc) return;
@@ -530,7 +530,7 @@ __global__ void geom_xc_kernel(int Nc, const int* __restrict__ cn_off, const int
 }
 
 // compute_xf (:44-59), compute_rf (:73-89), compute_nf (:91-116), compute_If (:118-125).
-__global__ void geom_face_kernel(int Nf, int F_BC, const int* __restrict__ fn_con, const int* __restrict__ fc_con,
+static __global__ void geom_face_kernel(int Nf, int F_BC, const int* __restrict__ fn_con, const int* __restrict__ fc_con,
                                  const double* __restrict__ nodes, const double* __restrict__ xc,
                                  FaceGeo<double>* __restrict__ geo) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -561,7 +561,7 @@ __global__ void geom_face_kernel(int Nf, int F_BC, const int* __restrict__ fn_co
 
 // compute_iv (:127-146) + zero_bc_iv (:148-154), gathered per cell over its faces in
 // increasing face order (the reference's scatter order for that cell).
-__global__ void geom_iv_kernel(int Nc, int F_BC, const int* __restrict__ cf_off, const int* __restrict__ cf_con,
+static __global__ void geom_iv_kernel(int Nc, int F_BC, const int* __restrict__ cf_off, const int* __restrict__ cf_con,
                                const int* __restrict__ fc_con, const FaceGeo<double>* __restrict__ geo,
                                double* __restrict__ iv) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -657,7 +657,7 @@ __global__ void in_kernel(int Nc, const double* __restrict__ in, const int* __re
 }
 
 // dst[i] = src[perm[i]]
-__global__ void permute_kernel(int n, const double* __restrict__ src, const int* __restrict__ perm,
+static __global__ void permute_kernel(int n, const double* __restrict__ src, const int* __restrict__ perm,
                                double* __restrict__ dst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = src[perm[i]];

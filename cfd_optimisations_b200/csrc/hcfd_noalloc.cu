@@ -1,0 +1,151 @@
+// hcfd_step_noalloc: one time step of the per-cell step kernels for callers that cannot
+// allocate device memory.
+//
+// Who needs it: code that runs where cudaMalloc is not allowed or not wanted — a host
+// framework that owns every byte of device memory through its own pool, a caller building
+// a stream that must not synchronise the device (cudaMalloc/cudaFree can), or a real-time
+// loop with a fixed memory budget.  Such a caller owns the inputs and outputs (state, face
+// records, cell->face slots, inverse areas) in its own device buffers; this entry point
+// adds no allocation of any kind.  The one buffer the step needs besides them — the limited
+// gradients that pass 1 writes and pass 2 reads, plus the reduction slots — is the static
+// device array below, sized for at most HCFD_NOALLOC_MAX_CELLS cells.  Every GPU that loads
+// the library holds that array (about 4 MiB) until the process exits.
+#include "hcfd_internal.hpp"
+#include "hcfd_kernels.cuh"
+
+#include <cmath>
+#include <mutex>
+#include <string>
+
+using hcfd::fail;
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kMaxBlocks = (HCFD_NOALLOC_MAX_CELLS + kBlock - 1) / kBlock;
+
+// Byte layout of the scratch array (offsets are multiples of 256).
+constexpr size_t kPhiG = 0;                                                   // Grad8<double> planes
+constexpr size_t kPartial = kPhiG + (size_t) 64 * HCFD_NOALLOC_MAX_CELLS;     // double[kMaxBlocks]
+constexpr size_t kDtmin = kPartial + ((sizeof(double) * kMaxBlocks + 255) & ~(size_t) 255);  // u64[2]
+constexpr size_t kCounter = kDtmin + 256;                                     // unsigned int
+constexpr size_t kStats = kCounter + 256;                                     // StepStats
+constexpr size_t kScratchBytes = kStats + 256;
+
+// The scratch.  In host code `g_noalloc_scratch` names a host-side stand-in, not device
+// memory: kernels get the device address taken by cudaGetSymbolAddress at set-up.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+unsigned char* g_addr[kMaxDevices] = {nullptr};
+std::mutex g_addr_mu;
+
+// Clears what must start at zero (and the dt minimum at +inf) on every call.
+__global__ void noalloc_reset_kernel(unsigned long long* dtmin, unsigned int* counter, hcfd::StepStats* stats) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        dtmin[0] = 0x7FF0000000000000ULL;
+        dtmin[1] = 0x7FF0000000000000ULL;
+        *counter = 0u;
+        hcfd::StepStats z{};
+        *stats = z;
+    }
+}
+
+template <int W>
+void launch(const hcfd::StepArgs<double>& a, cudaStream_t st) {
+    const int grid = (a.Nc + kBlock - 1) / kBlock;
+    hcfd::pass1_kernel<double, W><<<grid, kBlock, 0, st>>>(a);
+    hcfd::pass2_kernel<double, W, false><<<grid, kBlock, 0, st>>>(a);
+}
+
+}  // namespace
+
+extern "C" int hcfd_step_noalloc(const hcfd_noalloc_mesh* m, const double* U_in, double* U_out, int time_mode,
+                                 double dt_or_cfl, void* stream, double* dt_used, double* res_l2) {
+    hcfd::clear_error();
+    if (!m || !U_in || !U_out || U_in == U_out || !m->slot || !m->geo || !m->iv)
+        return fail(HCFD_EINVAL, "step_noalloc: null or aliased argument");
+    if (m->Nc <= 0 || m->Nc > HCFD_NOALLOC_MAX_CELLS)
+        return fail(HCFD_EINVAL, "step_noalloc: Nc must be in 1.." + std::to_string(HCFD_NOALLOC_MAX_CELLS) +
+                                     " (the size of the static scratch)");
+    if (m->Nf <= 0 || m->F_BC < 0 || m->F_BC > m->Nf || (m->slots != 3 && m->slots != 4 && m->slots != 8) ||
+        m->nbc < 0 || m->nbc > hcfd::MAXBC || (m->nbc > 0 && (!m->bc_first || !m->bc_type || !m->bc_state)) ||
+        !(m->gma > 1.0) || (m->limiter != HCFD_LIMITER_BJ && m->limiter != HCFD_LIMITER_VENKAT) ||
+        time_mode < HCFD_FIXED_DT || time_mode > HCFD_GLOBAL_CFL || !std::isfinite(dt_or_cfl) || dt_or_cfl < 0)
+        return fail(HCFD_EINVAL, "step_noalloc: bad argument");
+
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("step_noalloc: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return fail(HCFD_EINVAL, "step_noalloc: device index too large");
+    unsigned char* base;
+    {
+        // Once per device, with that device current: the device address of the scratch.
+        std::lock_guard<std::mutex> lk(g_addr_mu);
+        if (!g_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p)
+                return fail(HCFD_ECUDA, std::string("step_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_addr[dev] = static_cast<unsigned char*>(p);
+        }
+        base = g_addr[dev];
+    }
+
+    hcfd::BCTable bc{};
+    bc.nbc = m->nbc;
+    for (int b = 0; b < m->nbc; b++) {
+        bc.F1[b] = m->bc_first[b];
+        bc.type[b] = m->bc_type[b];
+        if (bc.type[b] < HCFD_SYMMETRY || bc.type[b] > HCFD_SUBOUTLET) return fail(HCFD_EINVAL, "step_noalloc: bad BC type");
+        const double* q = m->bc_state + 4 * b;
+        for (int v = 0; v < 4; v++) bc.QBC[b][v] = q[v];
+        // primitive -> conservative, BoundaryCondition::init (src/Base/BoundaryConditions/Base.cpp:18-22)
+        bc.UBC[b][0] = q[0];
+        for (int v = 1; v < 4; v++) bc.UBC[b][v] = q[0] * q[v];
+        bc.UBC[b][3] = q[3] / (m->gma - 1) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2]);
+    }
+    bc.F1[m->nbc] = m->nbc > 0 ? m->bc_first[m->nbc] : m->Nf;
+
+    hcfd::StepArgs<double> a;
+    a.U = reinterpret_cast<const hcfd::Cell4<double>*>(U_in);
+    a.Unew = reinterpret_cast<hcfd::Cell4<double>*>(U_out);
+    a.phiG = reinterpret_cast<hcfd::Grad8<double>*>(base + kPhiG);
+    a.geo = reinterpret_cast<const hcfd::FaceGeo<double>*>(m->geo);
+    a.slot = reinterpret_cast<const int2*>(m->slot);
+    a.iv = m->iv;
+    a.dtmin = reinterpret_cast<unsigned long long*>(base + kDtmin);
+    a.dtmin_next = a.dtmin + 1;
+    a.partial = reinterpret_cast<double*>(base + kPartial);
+    a.counter = reinterpret_cast<unsigned int*>(base + kCounter);
+    a.stats = reinterpret_cast<hcfd::StepStats*>(base + kStats);
+    a.Nc = m->Nc;
+    a.F_BC = m->F_BC;
+    a.limiter = m->limiter;
+    a.time_mode = time_mode;
+    a.gma = m->gma;
+    a.venkat_K = m->venkat_K;
+    a.dt_or_cfl = dt_or_cfl;
+    a.bc = bc;
+
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    noalloc_reset_kernel<<<1, 32, 0, st>>>(a.dtmin, a.counter, a.stats);
+    switch (m->slots) {
+    case 3: launch<3>(a, st); break;
+    case 4: launch<4>(a, st); break;
+    default: launch<8>(a, st); break;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("step_noalloc: launch: ") + cudaGetErrorString(e));
+    if (dt_used || res_l2) {
+        hcfd::StepStats h{};
+        e = cudaMemcpyAsync(&h, a.stats, sizeof(h), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("step_noalloc: ") + cudaGetErrorString(e));
+        const int nreal = m->Nc - (m->Nf - m->F_BC);
+        if (dt_used) *dt_used = h.dt_last;
+        if (res_l2) *res_l2 = nreal > 0 ? std::sqrt(h.res2_last / nreal) : 0.0;
+        if (h.nonfinite) return fail(HCFD_ENONFINITE, "step_noalloc: a NaN or Inf appeared");
+    }
+    return HCFD_OK;
+}

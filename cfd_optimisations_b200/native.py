@@ -48,6 +48,16 @@ class StepStats(ct.Structure):
                 ("steps", ct.c_longlong), ("nonfinite", ct.c_int)]
 
 
+class NoallocMesh(ct.Structure):
+    _fields_ = [("Nc", ct.c_int), ("Nf", ct.c_int), ("F_BC", ct.c_int), ("slots", ct.c_int),
+                ("slot", ct.c_void_p), ("geo", ct.c_void_p), ("iv", ct.c_void_p),
+                ("nbc", ct.c_int), ("bc_first", _ip), ("bc_type", _ip), ("bc_state", _dp),
+                ("gma", ct.c_double), ("limiter", ct.c_int), ("venkat_K", ct.c_double)]
+
+
+NOALLOC_MAX_CELLS = 65536
+
+
 class HcfdError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"hcfd error {code}: {msg}")
@@ -85,6 +95,8 @@ _SIGS = {
     "hcfd_host_unpin": (ct.c_int, [ct.c_void_p]),
     "hcfd_write_hsln": (ct.c_int, [ct.c_char_p, ct.c_int, ct.POINTER(ct.c_char_p), ct.c_int, ct.POINTER(_dp)]),
     "hcfd_plan_check": (ct.c_int, [ct.POINTER(MeshView), ct.c_int, ct.c_int, ct.POINTER(ct.c_longlong)]),
+    "hcfd_step_noalloc": (ct.c_int, [ct.POINTER(NoallocMesh), ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_double,
+                                     ct.c_void_p, _dp, _dp]),
     "hcfd_set_device": (ct.c_int, [ct.c_int, _ip]),
     "hcfd_device_sync": (ct.c_int, []),
     "hcfd_last_error": (ct.c_char_p, []),

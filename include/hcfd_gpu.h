@@ -216,6 +216,52 @@ int  hcfd_host_unpin(void* p);
  * face entries, slots per cell, total halo cells.  No reference counterpart. */
 int  hcfd_plan_check(const hcfd_mesh_view* mesh, int tile, int keep_numbering, long long* info);
 
+/* ---- one step without device allocation -------------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc: a framework
+ * that owns all device memory through its own pool, a caller that must not let a library
+ * allocate (cudaMalloc and cudaFree can synchronise the device), or a loop with a fixed
+ * memory budget.  The caller owns every input and output in its own device buffers; the
+ * only other memory the step needs (the limited gradients between its two passes and the
+ * reduction slots) is a static device array of the library, sized for at most
+ * HCFD_NOALLOC_MAX_CELLS cells (about 4 MiB, held on every GPU that loads the library until
+ * the process exits).  Larger meshes are rejected with HCFD_EINVAL. */
+#define HCFD_NOALLOC_MAX_CELLS 65536
+
+typedef struct hcfd_noalloc_mesh {
+    int Nc;                 /* cells, ghosts included (1..HCFD_NOALLOC_MAX_CELLS)                 */
+    int Nf;                 /* faces                                                              */
+    int F_BC;               /* first boundary face (faces F_BC..Nf-1 have a ghost on the right)   */
+    int slots;              /* face slots per cell: 3, 4 or 8                                     */
+    const int* slot;        /* device, slots x Nc int pairs, slot-major: slot k of cell c at
+                               2 (k Nc + c): {face f if c is the face's left cell, else ~f;
+                               the other cell}; unused slots {-1, -1}; a ghost cell's first slot
+                               is unused.  Each cell's faces in increasing face index.          */
+    const double* geo;      /* device, Nf x 8: nx, ny, length, If, rLx, rLy, rRx, rRy (the
+                               reference's Domain arrays, src/Base/Domain.hpp:15-24)             */
+    const double* iv;       /* device, Nc: 1/area, 0 for ghost cells                               */
+    int nbc;                /* boundary colours (0..16)                                           */
+    const int* bc_first;    /* host, nbc + 1: first face of each boundary colour, then Nf         */
+    const int* bc_type;     /* host, nbc: enum hcfd_bctype                                        */
+    const double* bc_state; /* host, nbc x 4: primitive (rho, u, v, p)                            */
+    double gma;
+    int limiter;            /* enum hcfd_limiter                                                  */
+    double venkat_K;
+} hcfd_noalloc_mesh;
+
+/* One step (HCFD_FIXED_DT or HCFD_GLOBAL_CFL) from U_in to U_out, both caller-owned device
+ * buffers of 4 Nc doubles that must not overlap, laid out as two planes of pairs: plane 0
+ * holds (rho, rho u) of cells 0..Nc-1, plane 1 (at offset 2 Nc) holds (rho v, E).  Work is
+ * enqueued on `stream` (a cudaStream_t, NULL for the default stream).  When dt_used or
+ * res_l2 is non-NULL the call waits for the stream and reports the step's dt and L2 density
+ * residual.  Allocates nothing: no cudaMalloc, cudaFree or allocating library call.
+ * The first call on each device looks up the device address of the static scratch; make
+ * that first call before any stream capture.  All calls share the one scratch array, which
+ * keeps the last call's contents: calls that overlap on the GPU (other streams, other
+ * threads) race and must be serialised by the caller. */
+int  hcfd_step_noalloc(const hcfd_noalloc_mesh* mesh, const double* U_in, double* U_out, int time_mode,
+                       double dt_or_cfl, void* stream, double* dt_used, double* res_l2);
+
 /* ---- output ------------------------------------------------------------------------- */
 
 /* Replaces Writer::write_soln (src/Writer.cpp:22-39): writes int32 Nc, nvars, nchars,
