@@ -121,12 +121,20 @@ def dist_setup(nproc: int):
 
 
 def allmax(dist, x: float) -> float:
+    """Maximum of x over the ranks (the slowest rank's time)."""
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate(units_per_rank: float, world: int, ms_max: float) -> float:
+    """Whole-job throughput: every rank processed the same units; the job took the slowest
+    rank's time."""
+    return units_per_rank * world / (ms_max * 1e-3)
 
 
 def barrier(dist):
@@ -283,7 +291,7 @@ def main():
     s.profile(False)
     st = s.stats()
     ms_max = allmax(dist, ms)
-    value = ntri * args.steps * world / (ms_max * 1e-3)
+    value = aggregate(ntri * args.steps, world, ms_max)
 
     # Roofline of the dominant kernel.  Algorithmic bytes (two-pass minimum, w = 8):
     #   pass 1: U (4w) + iv (w) + phiG (8w) per cell, (8 + 7w) per face

@@ -1,0 +1,54 @@
+"""The C ABI library (CPU only): it loads without a GPU, exports every function declared in
+include/*.h, and its host-only entry points work.  No compute call is made here."""
+import ctypes as ct
+import os
+import re
+import subprocess
+
+import pytest
+
+import cfd_optimisations_b200 as H
+from cfd_optimisations_b200 import native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if not fn.endswith(".h"):
+            continue
+        with open(os.path.join(ROOT, "include", fn)) as fh:
+            src = re.sub(r"/\*.*?\*/", "", fh.read(), flags=re.S)
+        names |= set(re.findall(r"\b(hcfd_[a-z0-9_]+)\s*\(", src))
+    return names
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared()
+    assert len(names) >= 30
+    out = subprocess.run(["nm", "-D", "--defined-only", N.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (hcfd_[a-z0-9_]+)\b", out))
+    assert names <= exported, sorted(names - exported)
+
+
+def test_python_binding_covers_the_abi():
+    assert declared() <= set(N._SIGS), sorted(declared() - set(N._SIGS))
+
+
+def test_library_loads_and_reports_errors():
+    L = N.lib()
+    # host-only paths: a bad mesh argument fails cleanly with a message
+    rc = L.hcfd_mesh_load(b"/nonexistent/file.hmsh", ct.byref(ct.c_void_p()))
+    assert rc == N.EIO
+    assert b"cannot open" in L.hcfd_last_error()
+    assert L.hcfd_gpu_create(None, None, ct.byref(ct.c_void_p())) == N.EINVAL
+
+
+def test_no_gpu_here_means_a_cuda_error_not_a_fallback():
+    if os.path.exists("/dev/nvidia0"):
+        pytest.skip("a GPU is present")
+    m = H.Mesh.wedge(11, 6, seed=1)
+    with pytest.raises(H.HcfdError) as e:
+        H.Solver(m)
+    assert e.value.code == N.ECUDA

@@ -1,0 +1,224 @@
+"""Pins of the CPU oracle (CPU only).
+
+The oracle (oracle/hcfd_oracle.c) restates the reference's Base solver; before it can judge
+the GPU it is checked here against the reference's own golden vectors (sols/Base_0.hsln,
+sols/Base_1.hsln, committed under tests/golden) and, where the reference has been compiled
+into oracle/_ref, against the reference itself on generated meshes.  The features the
+reference lacks (CFL dt, local dt, Venkatakrishnan, residual norm, wall Cp) are checked
+against independent numpy restatements on small cases.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cfd_optimisations_b200 as H
+import oracle as O
+
+
+def wedge_case_ref():
+    # src/Test.cpp:51-64
+    gma, M = 1.4, 2.0
+    p = 1.0 / (gma * M * M)
+    q = np.array([1.0, 1.0, 0.0, p])
+    return np.array([0, 0, 0, 2, 4]), np.tile(q, (4, 1)), q
+
+
+@pytest.fixture(scope="module")
+def wedge(golden):
+    return O.read_hmsh(os.path.join(golden, "wedge.hmsh"))
+
+
+def test_reader_facts(wedge):
+    assert (wedge["dim"], wedge["Nn"], wedge["Ncol"], wedge["NBCcol"], wedge["Nc"], wedge["Nf"]) == \
+        (2, 3621, 5, 4, 3740, 7120)
+    assert list(wedge["coloff"]) == [0, 6880, 6950, 7020, 7070, 7120]
+    assert wedge["pnames"] == ["upper", "lower", "inlet", "outlet"]
+
+
+def test_oracle_reproduces_base0_and_base1_bit_for_bit(wedge, golden):
+    bcmap, qbc, q = wedge_case_ref()
+    o = O.Oracle(wedge)
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    _, b0 = O.read_hsln(os.path.join(golden, "Base_0.hsln"))
+    names, b1 = O.read_hsln(os.path.join(golden, "Base_1.hsln"))
+    assert names == ["Density", "Velocity_X", "Velocity_Y", "Pressure"]
+    assert np.array_equal(o.Q(), b0)
+    # run(1.0, 1e-3, 1.0): t accumulates 1e-3 to 1.0000000000000007 >= 1 after exactly 1000 steps
+    t, n = 0.0, 0
+    while t < 1.0:
+        t += 1e-3
+        n += 1
+    assert n == 1000
+    for _ in range(n):
+        o.step(O.FIXED_DT, 1e-3)
+    assert np.array_equal(o.Q(), b1)
+
+
+@pytest.mark.skipif(not O.RefSolver.available(), reason="reference not compiled into oracle/_ref")
+def test_reference_build_reproduces_goldens(golden):
+    bcmap, qbc, q = wedge_case_ref()
+    path = os.path.join(golden, "wedge.hmsh")
+    _, b1 = O.read_hsln(os.path.join(golden, "Base_1.hsln"))
+    for layout in ("Base", "SoA"):
+        r = O.RefSolver(path, bcmap, qbc, q, layout=layout)
+        r.steps(1000, 1e-3)
+        assert np.array_equal(r.Q(), b1), layout
+
+
+@pytest.mark.skipif(not O.RefSolver.available(), reason="reference not compiled into oracle/_ref")
+@pytest.mark.parametrize("numbering", [H.NUMBER_NATURAL, H.NUMBER_RANDOM, H.NUMBER_RCM, H.NUMBER_MORTON])
+def test_oracle_matches_reference_on_generated_meshes(tmp_path, numbering):
+    m = H.Mesh.wedge(41, 21, seed=3, numbering=numbering)
+    path = str(tmp_path / "w.hmsh")
+    m.write(path)
+    bcmap, qbc, q = H.wedge_case(2.5)
+    o = O.Oracle(O.read_hmsh(path))
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    r = O.RefSolver(path, bcmap, qbc, q)
+    for _ in range(10):
+        o.step(O.FIXED_DT, 2e-3)
+    r.steps(10, 2e-3)
+    assert np.array_equal(o.U(), r.U())
+
+
+@pytest.mark.skipif(not O.RefSolver.available(), reason="reference not compiled into oracle/_ref")
+def test_oracle_phases_match_reference_phases(golden):
+    """Gradient, limiter and residual arrays, phase by phase (Euler.cpp:86-96)."""
+    path = os.path.join(golden, "wedge.hmsh")
+    bcmap, qbc, q = wedge_case_ref()
+    o = O.Oracle(O.read_hmsh(path))
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    r = O.RefSolver(path, bcmap, qbc, q)
+    for _ in range(50):
+        o.step(O.FIXED_DT, 1e-3)
+    r.steps(50, 1e-3)
+    for ph in range(4):
+        o.phase(ph)
+        r.phase(ph)
+    assert np.array_equal(o.get(O.F_G), r.G())
+    assert np.array_equal(o.get(O.F_PHI), r.get(2))
+    assert np.array_equal(o.get(O.F_R), r.get(3))
+
+
+def _numpy_local_dt(m, dom, U, gma=1.4):
+    """Independent restatement of the oracle's local time step at CFL 1."""
+    fc = m["fc_con"].reshape(-1, 2)
+    nf, Af, iv = dom["nf"], dom["Af"], dom["iv"]
+    lam = np.zeros(m["Nc"])
+    r, ru, rv, E = U
+    u, v = ru / r, rv / r
+    p = (gma - 1) * (E - 0.5 * (ru * u + rv * v))
+    a = np.sqrt(gma * p / r)
+    for side in (0, 1):
+        c = fc[:, side]
+        lam += np.bincount(c, weights=(np.abs(u[c] * nf[:, 0] + v[c] * nf[:, 1]) + a[c]) * Af, minlength=m["Nc"])
+    real = iv != 0
+    dt = np.zeros(m["Nc"])
+    dt[real] = 1.0 / (iv[real] * lam[real])
+    return dt
+
+
+def test_cfl_dt_matches_numpy_restatement():
+    m = H.Mesh.wedge(41, 21, seed=8, numbering=H.NUMBER_RANDOM).arrays()
+    bcmap, qbc, q = H.wedge_case(2.5)
+    o = O.Oracle(m)
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    for _ in range(5):
+        o.step(O.GLOBAL_CFL, 0.5)
+    dom = o.domain()
+    dt_np = _numpy_local_dt(m, dom, o.U())
+    dt_or = o.get(O.F_DTLOC)
+    np.testing.assert_allclose(dt_or, dt_np, rtol=1e-12)
+    dt_used, _ = o.step(O.GLOBAL_CFL, 0.5)
+    assert dt_used == pytest.approx(0.5 * dt_np[dom["iv"] != 0].min(), rel=1e-12)
+
+
+def test_local_time_stepping_uses_each_cells_dt():
+    m = H.Mesh.wedge(41, 21, seed=8).arrays()
+    bcmap, qbc, q = H.wedge_case(2.5)
+    o = O.Oracle(m)
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    o.step(O.GLOBAL_CFL, 0.5)
+    U0 = o.U()
+    dt = 0.5 * o.get(O.F_DTLOC)
+    for ph in range(4):
+        o.phase(ph)
+    R = o.get(O.F_R)
+    o.phase(5)
+    o.set_U(U0)
+    o.step(O.LOCAL_CFL, 0.5)
+    U1 = o.U()
+    real = o.get(O.F_IV) != 0
+    np.testing.assert_allclose(U1[:, real], (U0 + dt * R)[:, real], rtol=1e-13, atol=1e-14)
+
+
+def test_residual_norm_definition():
+    m = H.Mesh.wedge(41, 21, seed=4).arrays()
+    bcmap, qbc, q = H.wedge_case(2.5)
+    o = O.Oracle(m)
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    for _ in range(3):
+        o.step(O.GLOBAL_CFL, 0.5)
+    U0 = o.U()
+    for ph in range(4):
+        o.phase(ph)
+    R = o.get(O.F_R)
+    o.phase(5)
+    o.set_U(U0)
+    _, res = o.step(O.GLOBAL_CFL, 0.5)
+    real = o.get(O.F_IV) != 0
+    assert res == pytest.approx(np.sqrt(np.sum(R[0, real] ** 2) / real.sum()), rel=1e-12)
+
+
+def test_venkatakrishnan_formula():
+    """With K = 0 (eps^2 = 0) the Venkatakrishnan face value is (y^2 + 2y)/(y^2 + y + 2),
+    y = D1/d; check it through a one-cell-patch comparison with a direct evaluation."""
+    m = H.Mesh.wedge(41, 21, seed=2).arrays()
+    bcmap, qbc, q = H.wedge_case(2.5)
+    o = O.Oracle(m)
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    for _ in range(20):
+        o.step(O.GLOBAL_CFL, 0.5)
+    o.set_limiter(O.VENKAT, 0.0)
+    o.phase(0)
+    o.phase(1)
+    phi = o.get(O.F_PHI)
+    G = o.get(O.F_G)
+    U = o.get(O.F_U)
+    dom = o.domain()
+    fc = m["fc_con"].reshape(-1, 2)
+    Nc = m["Nc"]
+    real = np.nonzero(dom["iv"] != 0)[0]
+    rng = np.random.default_rng(0)
+    for c in rng.choice(real, 40, replace=False):
+        faces = [f for f in range(m["Nf"]) if c in fc[f]]
+        for v in range(4):
+            nb = [fc[f][1] if fc[f][0] == c else fc[f][0] for f in faces]
+            umax, umin = max(U[v, c], *U[v, nb]), min(U[v, c], *U[v, nb])
+            want = 1.0
+            for f in faces:
+                side = 0 if fc[f][0] == c else 1
+                d = G[v, 0, c] * dom["rf"][f, side, 0] + G[v, 1, c] * dom["rf"][f, side, 1]
+                if abs(d) > 1e-9:
+                    y = ((umax if d > 0 else umin) - U[v, c]) / d
+                    want = min(want, min(1.0, (y * y + 2 * y) / (y * y + y + 2)))
+            assert phi[v, c] == pytest.approx(want, rel=1e-12, abs=1e-14)
+
+
+def test_wall_cp_of_uniform_flow_is_zero():
+    m = H.Mesh.wedge(41, 21, seed=2).arrays()
+    bcmap, qbc, q = H.wedge_case(2.5)
+    o = O.Oracle(m)
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    cp = o.wall_cp(2, 1.4, 1.0, 2.5)
+    assert cp.size == 40
+    assert np.abs(cp).max() < 1e-14
