@@ -1,0 +1,98 @@
+"""Precision study: the FP32 path (float state, gradients, limiter and fluxes, compensated
+per-cell residual sums, double geometry and residual norm) against the FP64 path on the
+same mesh, both on the GPU, both run to convergence.
+
+    python -m cfd_optimisations_b200.precision [--nx 1025 --ny 513 --mach 3.0 --theta 20
+                                                 --cfl 0.8 --orders 8 --max-steps 50000]
+
+Defaults are the 1025 x 513-node wedge (1,048,576 triangles), M 3.0, ramp 20 degrees, local
+time stepping at CFL 0.8, stop when the L2 density residual has dropped `orders` orders
+below its first value or after `max-steps`.  Prints one JSON object: for each precision the
+steps and device time to convergence, and the FP32 errors against FP64 — relative L-inf and
+L2 of each conserved variable, and the L-inf and L2 error of the wall pressure coefficient
+on the lower wall (the ramp).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import (FP32, FP64, GLOBAL_CFL, LIMITER_BJ, LOCAL_CFL, NUMBER_RANDOM, Mesh, Solver, wedge_case)
+
+LOWER_WALL = 2   # colour of the lower wall (the ramp) in the generated wedge
+
+
+def converge(mesh: Mesh, precision: int, mach: float, cfl: float, orders: float, max_steps: int,
+             mode: int = LOCAL_CFL, limiter: int = LIMITER_BJ, chunk: int = 200) -> dict:
+    """Runs one solve to convergence; returns its state, wall Cp and timing."""
+    bcmap, qbc, q = wedge_case(mach)
+    s = Solver(mesh, limiter=limiter, precision=precision)
+    s.gather_bcs(bcmap, qbc)
+    s.initialise(q)
+    steps, ms, hist = 0, 0.0, []
+    st = s.step(1, mode, cfl)
+    steps += 1
+    res0 = st["res_first"]
+    while steps < max_steps:
+        n = min(chunk, max_steps - steps)
+        ms += s.step_timed(n, mode, cfl)
+        steps += n
+        st = s.stats()
+        hist.append((steps, st["res_l2"]))
+        if st["nonfinite"] or st["res_l2"] <= res0 * 10.0 ** (-orders):
+            break
+    rho, p = q[0], q[3]
+    speed = float(np.hypot(q[1], q[2]))
+    return dict(U=s.U(), cp=s.wall_cp(LOWER_WALL, rho, p, speed), steps=steps, ms=ms, res0=res0,
+                res=st["res_l2"], drop=float(np.log10(res0 / st["res_l2"])) if st["res_l2"] > 0 else None,
+                history=hist)
+
+
+def errors(a: dict, b: dict) -> dict:
+    """Errors of solve `a` against reference solve `b`."""
+    Ua, Ub = a["U"], b["U"]
+    den = np.abs(Ub).max(axis=1)
+    linf = (np.abs(Ua - Ub).max(axis=1) / den).tolist()
+    l2 = (np.sqrt(((Ua - Ub) ** 2).mean(axis=1)) / np.sqrt((Ub ** 2).mean(axis=1))).tolist()
+    dcp = a["cp"] - b["cp"]
+    return dict(rel_linf=linf, rel_l2=l2, cp_linf=float(np.abs(dcp).max()),
+                cp_l2=float(np.sqrt((dcp ** 2).mean())), cp_range=float(b["cp"].max() - b["cp"].min()))
+
+
+def study(nx=1025, ny=513, mach=3.0, theta=20.0, cfl=0.8, orders=8.0, max_steps=50000, seed=1234,
+          mode=LOCAL_CFL) -> dict:
+    mesh = Mesh.wedge(nx, ny, theta_deg=theta, seed=seed, numbering=NUMBER_RANDOM)
+    out = dict(workload=dict(nx=nx, ny=ny, triangles=2 * (nx - 1) * (ny - 1), mach=mach, theta_deg=theta, cfl=cfl,
+                             time_mode="local" if mode == LOCAL_CFL else "global", orders=orders,
+                             max_steps=max_steps))
+    runs = {}
+    for name, prec in (("fp64", FP64), ("fp32", FP32)):
+        t0 = time.perf_counter()
+        runs[name] = converge(mesh, prec, mach, cfl, orders, max_steps, mode=mode)
+        r = runs[name]
+        out[name] = dict(steps=r["steps"], device_ms=r["ms"], wall_s=time.perf_counter() - t0,
+                         residual_drop_orders=r["drop"], converged=bool(r["drop"] is not None and r["drop"] >= orders))
+    out["fp32_vs_fp64"] = errors(runs["fp32"], runs["fp64"])
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nx", type=int, default=1025)
+    ap.add_argument("--ny", type=int, default=513)
+    ap.add_argument("--mach", type=float, default=3.0)
+    ap.add_argument("--theta", type=float, default=20.0)
+    ap.add_argument("--cfl", type=float, default=0.8)
+    ap.add_argument("--orders", type=float, default=8.0)
+    ap.add_argument("--max-steps", type=int, default=50000)
+    ap.add_argument("--global-dt", action="store_true", help="global instead of local time stepping")
+    a = ap.parse_args()
+    print(json.dumps(study(a.nx, a.ny, a.mach, a.theta, a.cfl, a.orders, a.max_steps,
+                           mode=GLOBAL_CFL if a.global_dt else LOCAL_CFL)))
+
+
+if __name__ == "__main__":
+    main()
