@@ -46,7 +46,8 @@ def test_library_loads_and_reports_errors():
 
 
 def test_no_gpu_here_means_a_cuda_error_not_a_fallback():
-    if os.path.exists("/dev/nvidia0"):
+    from conftest import gpu_available
+    if gpu_available():
         pytest.skip("a GPU is present")
     m = H.Mesh.wedge(11, 6, seed=1)
     with pytest.raises(H.HcfdError) as e:
