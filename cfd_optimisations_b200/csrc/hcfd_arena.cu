@@ -1,0 +1,661 @@
+// Batched and served solves: many meshes packed into one flat device arena.
+//
+// The arena owns one set of device arrays sized from an HBM budget: cell planes (two
+// state buffers, limited gradients, 1/area, slot tables), face-entry blocks (records and
+// metadata) and halo lists.  Each admitted mesh (an instance) gets contiguous ranges in
+// each (first-fit free lists on the host, so per-instance offsets), its own tile plan
+// (hcfd_plan.cpp) with offsets added, its own BC table, dt or CFL number, dt minimum and
+// statistics.  The tiled step kernels (hcfd_tile.cuh) run in arena mode over the list of
+// all active tiles; a finalize kernel then forms each instance's residual from its tiles in
+// tile order.  An instance's arithmetic is exactly that of the single-mesh solver with the
+// same tile size, whatever else is in the arena, so a result is the same alone and in the
+// mix.  A chunk of steps is captured once as a CUDA graph and replayed until the set of
+// instances changes.
+#include "hcfd_internal.hpp"
+#include "hcfd_kernels.cuh"
+#include "hcfd_tile.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <memory>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+using hcfd::fail;
+using hcfd::Cell4;
+
+namespace {
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(HCFD_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+inline int nblk(long long n, int b) { return (int) ((n + b - 1) / b); }
+
+// First-fit allocator over [0, capacity) with coalescing free list.
+struct FreeList {
+    std::map<size_t, size_t> free_;   // offset -> length
+    size_t cap = 0, used = 0;
+    void init(size_t capacity) { free_.clear(); cap = capacity; used = 0; if (cap) free_[0] = cap; }
+    bool alloc(size_t n, size_t& off) {
+        if (n == 0) { off = 0; return true; }
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= n) {
+                off = it->first;
+                const size_t rest = it->second - n;
+                free_.erase(it);
+                if (rest) free_[off + n] = rest;
+                used += n;
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(size_t off, size_t n) {
+        if (n == 0) return;
+        used -= n;
+        auto it = free_.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) { it->second += nx->second; free_.erase(nx); }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) { pv->second += it->second; free_.erase(it); }
+        }
+    }
+};
+
+struct Inst {
+    bool active = false;
+    int Nc = 0, Nf = 0, Nreal = 0, ntiles = 0;
+    size_t c0 = 0, ncell = 0, e0 = 0, ne = 0, h0 = 0, nh = 0;
+    int* d_perm = nullptr;                 // instance internal -> input cell number
+    std::vector<int> tiles;                // 8 ints per tile, arena offsets
+    double dt = 0;
+    long long admitted_step = 0;
+};
+
+// Per active instance: its slot and its tile range in the active list.
+__global__ void arena_finalize_kernel(int nact, const int4* __restrict__ act, const double* __restrict__ tile_r2,
+                                      const int* __restrict__ tile_bad, const double* __restrict__ inst_dt,
+                                      unsigned long long* inst_dtmin, hcfd::StepStats* stats, int time_mode, int par) {
+    const int i = blockIdx.x;
+    if (i >= nact) return;
+    const int4 d = act[i];
+    const int slot = d.x, t0 = d.y, t1 = d.z;
+    const int lane = threadIdx.x;
+    double x = 0.0;
+    int b = 0;
+    for (int t = t0 + lane; t < t1; t += 32) { x += tile_r2[t]; b |= tile_bad[t]; }
+    x = hcfd::warp_sum(x);
+    b = __any_sync(0xffffffffu, b);
+    if (lane == 0) {
+        hcfd::StepStats* st = stats + slot;
+        st->res2_last = x;
+        if (st->steps == 0) st->res2_first = x;
+        st->steps += 1;
+        const double v = inst_dt[slot];
+        st->dt_last = time_mode == hcfd::TM_FIXED ? v : v * __longlong_as_double((long long) inst_dtmin[2 * slot + par]);
+        if (b || !(x == x) || x > 1.7e308) st->nonfinite = 1;
+        inst_dtmin[2 * slot + (1 - par)] = 0x7FF0000000000000ULL;
+    }
+}
+
+template <class T>
+__global__ void arena_fill_kernel(size_t ps, size_t c0, int n, Cell4<T>* U, double u0, double u1, double u2, double u3) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T u[4] = {T(u0), T(u1), T(u2), T(u3)};
+    hcfd::st_cell(U, ps, (int) (c0 + i), u);
+}
+
+template <class T>
+__global__ void arena_out_kernel(size_t ps, size_t c0, int n, const Cell4<T>* __restrict__ U, const int* __restrict__ perm,
+                                 double gma, int prims, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T t[4];
+    hcfd::ld_cell(U, ps, (int) (c0 + i), t);
+    const size_t j = perm[i];
+    const double u0 = t[0], u1 = t[1], u2 = t[2], u3 = t[3];
+    if (!prims) {
+        out[j] = u0; out[(size_t) n + j] = u1; out[2 * (size_t) n + j] = u2; out[3 * (size_t) n + j] = u3;
+        return;
+    }
+    const double q1 = u1 / u0, q2 = u2 / u0;
+    out[j] = u0; out[(size_t) n + j] = q1; out[2 * (size_t) n + j] = q2;
+    out[3 * (size_t) n + j] = (gma - 1) * (u3 - 0.5 * u0 * (q1 * q1 + q2 * q2));
+}
+
+template <class T>
+__global__ void arena_iv_kernel(int n, const double* __restrict__ ivu, const int* __restrict__ perm, T* __restrict__ iv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) iv[i] = T(ivu[perm[i]]);
+}
+
+}  // namespace
+
+
+struct hcfd_arena {
+    hcfd_arena_params prm{};
+    int device = 0, nsm = 0;
+    cudaStream_t stream = nullptr;
+    int B = 128, W = 3, Wp = 4, Hcap = 112, Fcap = 288;
+    size_t Ccap = 0, Ecap = 0, HLcap = 0;
+    FreeList fc, fe, fh;
+    size_t tsz = 8;
+    // device arrays
+    void* U[2] = {nullptr, nullptr};
+    void* phiG = nullptr;
+    void* iv = nullptr;
+    short* cslot = nullptr;
+    void* tgeo = nullptr;
+    short* tmeta = nullptr;
+    int* halo = nullptr;
+    double* inst_dt = nullptr;
+    unsigned long long* inst_dtmin = nullptr;
+    hcfd::BCTable* inst_bc = nullptr;
+    hcfd::StepStats* stats = nullptr;
+    int4* tiles = nullptr;
+    int4* act = nullptr;
+    double* tile_r2 = nullptr;
+    int* tile_bad = nullptr;
+    unsigned int* err = nullptr;
+    size_t tiles_cap = 0;
+    // host
+    std::vector<Inst> inst;
+    int nact_tiles = 0, nact = 0;
+    int cur = 0, par = 0;
+    int time_mode = HCFD_GLOBAL_CFL;
+    size_t smem1 = 0, smem2 = 0;
+    int grid1 = 0, grid2 = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    long long steps_done = 0;
+    bool fp32() const { return prm.precision == HCFD_FP32; }
+};
+
+namespace {
+
+void free_graph(hcfd_arena* a) {
+    if (a->graph) { cudaGraphExecDestroy(a->graph); a->graph = nullptr; a->graph_steps = 0; }
+}
+
+template <class T>
+hcfd::TileArgs<T> arena_args(hcfd_arena* A, int cur, int par) {
+    hcfd::TileArgs<T> a{};
+    hcfd::StepArgs<T>& s = a.s;
+    s.U = (const Cell4<T>*) A->U[cur];
+    s.Unew = (Cell4<T>*) A->U[1 - cur];
+    s.phiG = (hcfd::Grad8<T>*) A->phiG;
+    s.iv = (const T*) A->iv;
+    s.Nc = (int) A->Ccap;
+    s.limiter = A->prm.limiter;
+    s.time_mode = A->time_mode;
+    s.gma = T(A->prm.gma);
+    s.venkat_K = T(A->prm.venkat_K);
+    a.tgeo = (const T*) A->tgeo;
+    a.tmeta = A->tmeta;
+    a.halo = A->halo;
+    a.cslot = A->cslot;
+    a.ntiles = A->nact_tiles;
+    a.B = A->B;
+    a.Wp = A->Wp;
+    a.Hmax = A->Hcap;
+    a.Fmax = A->Fcap;
+    a.err = A->err;
+    a.ps = (int) A->Ccap;
+    a.tiles = A->tiles;
+    a.inst_dt = A->inst_dt;
+    a.inst_dtmin = A->inst_dtmin;
+    a.inst_bc = A->inst_bc;
+    a.tile_r2 = A->tile_r2;
+    a.tile_bad = A->tile_bad;
+    a.par = par;
+    return a;
+}
+
+template <class T, int W>
+int enqueue_step(hcfd_arena* A, int cur, int par) {
+    hcfd::TileArgs<T> a = arena_args<T>(A, cur, par);
+    constexpr bool COMP = std::is_same<T, float>::value;
+    hcfd::tile_pass1_kernel<T, W, true><<<A->grid1, A->B + 32, A->smem1, A->stream>>>(a);
+    hcfd::tile_pass2_kernel<T, W, COMP, true><<<A->grid2, A->B + 32, A->smem2, A->stream>>>(a);
+    arena_finalize_kernel<<<A->nact, 32, 0, A->stream>>>(A->nact, A->act, A->tile_r2, A->tile_bad, A->inst_dt,
+                                                         A->inst_dtmin, A->stats, A->time_mode, par);
+    CK(cudaGetLastError());
+    return HCFD_OK;
+}
+
+template <class T>
+int enqueue_step_w(hcfd_arena* A, int cur, int par) {
+    return A->W == 3 ? enqueue_step<T, 3>(A, cur, par) : enqueue_step<T, 4>(A, cur, par);
+}
+
+template <class T, int W>
+int setup_kernels(hcfd_arena* A) {
+    constexpr bool COMP = std::is_same<T, float>::value;
+    A->smem1 = hcfd::TileSmem<T>(A->B, A->Hcap, A->Fcap, W, A->Wp, false).total;
+    A->smem2 = hcfd::TileSmem<T>(A->B, A->Hcap, A->Fcap, W, A->Wp, true).total;
+    int maxsm = 0;
+    CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, A->device));
+    if ((int) A->smem2 > maxsm) return fail(HCFD_EINVAL, "arena: tile does not fit in shared memory");
+    CK(cudaFuncSetAttribute(hcfd::tile_pass1_kernel<T, W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) A->smem1));
+    CK(cudaFuncSetAttribute(hcfd::tile_pass2_kernel<T, W, COMP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) A->smem2));
+    int b1 = 0, b2 = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, hcfd::tile_pass1_kernel<T, W, true>, A->B + 32, A->smem1));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, hcfd::tile_pass2_kernel<T, W, COMP, true>, A->B + 32, A->smem2));
+    if (b1 < 1 || b2 < 1) return fail(HCFD_EINVAL, "arena: kernels cannot be resident");
+    A->grid1 = b1 * A->nsm;
+    A->grid2 = b2 * A->nsm;
+    return HCFD_OK;
+}
+
+// Rebuilds the active tile list and the per-instance tile ranges, in slot order.
+int rebuild_active(hcfd_arena* A) {
+    std::vector<int> tl;
+    std::vector<int4> act;
+    for (size_t k = 0; k < A->inst.size(); k++) {
+        const Inst& I = A->inst[k];
+        if (!I.active) continue;
+        const int t0 = (int) (tl.size() / 8);
+        tl.insert(tl.end(), I.tiles.begin(), I.tiles.end());
+        act.push_back(make_int4((int) k, t0, (int) (tl.size() / 8), 0));
+    }
+    A->nact_tiles = (int) (tl.size() / 8);
+    A->nact = (int) act.size();
+    if ((size_t) A->nact_tiles > A->tiles_cap) return fail(HCFD_EINVAL, "arena: tile list capacity exceeded");
+    if (!tl.empty()) CK(cudaMemcpyAsync(A->tiles, tl.data(), sizeof(int) * tl.size(), cudaMemcpyHostToDevice, A->stream));
+    if (!act.empty()) CK(cudaMemcpyAsync(A->act, act.data(), sizeof(int4) * act.size(), cudaMemcpyHostToDevice, A->stream));
+    CK(cudaStreamSynchronize(A->stream));
+    free_graph(A);
+    return HCFD_OK;
+}
+
+template <class P>
+int dalloc(P** p, size_t n) {
+    cudaError_t e = cudaMalloc((void**) p, std::max<size_t>(n, 1) * sizeof(P));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(e == cudaErrorMemoryAllocation ? HCFD_ENOMEM : HCFD_ECUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return HCFD_OK;
+}
+
+void arena_free(hcfd_arena* A) {
+    if (!A) return;
+    cudaSetDevice(A->device);
+    if (A->stream) cudaStreamSynchronize(A->stream);
+    free_graph(A);
+    for (auto& I : A->inst) if (I.d_perm) cudaFree(I.d_perm);
+    void* p[] = {A->U[0], A->U[1], A->phiG, A->iv, A->cslot, A->tgeo, A->tmeta, A->halo, A->inst_dt, A->inst_dtmin,
+                 A->inst_bc, A->stats, A->tiles, A->act, A->tile_r2, A->tile_bad, A->err};
+    for (void* q : p) if (q) cudaFree(q);
+    if (A->stream) cudaStreamDestroy(A->stream);
+}
+
+void prim_to_cons(const double* q, double gma, double* u) {
+    u[0] = q[0];
+    for (int v = 1; v < 4; v++) u[v] = q[0] * q[v];
+    u[3] = q[3] / (gma - 1) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2]);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
+    hcfd::clear_error();
+    if (!prm || !out) return fail(HCFD_EINVAL, "arena_create: null argument");
+    *out = nullptr;
+    const hcfd_arena_params& p = *prm;
+    if (p.hbm_budget < ((size_t) 16 << 20) || !(p.gma > 1.0) || (p.precision != HCFD_FP64 && p.precision != HCFD_FP32) ||
+        (p.limiter != HCFD_LIMITER_BJ && p.limiter != HCFD_LIMITER_VENKAT) || p.max_instances < 1 ||
+        p.max_instances > 65536 || p.tile < 0 || p.tile > 256 || (p.tile % 32) || (p.slots != 0 && p.slots != 3 && p.slots != 4) ||
+        (p.time_mode != HCFD_FIXED_DT && p.time_mode != HCFD_GLOBAL_CFL && p.time_mode != HCFD_LOCAL_CFL))
+        return fail(HCFD_EINVAL, "arena_create: bad parameters");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(HCFD_ECUDA, "arena_create: no CUDA device");
+    auto A = std::make_unique<hcfd_arena>();
+    A->prm = p;
+    CK(cudaGetDevice(&A->device));
+    CK(cudaDeviceGetAttribute(&A->nsm, cudaDevAttrMultiProcessorCount, A->device));
+    A->B = p.tile ? p.tile : 128;
+    A->W = p.slots == 4 ? 4 : 3;
+    A->Wp = 4;
+    A->time_mode = p.time_mode;
+    // per-tile staging capacities (generous for triangle and quad meshes at this tile size)
+    A->Hcap = A->B * 7 / 8 + 16;
+    A->Fcap = A->B * 9 / 4 + 16;
+    A->tsz = A->fp32() ? 4 : 8;
+    const size_t ts = A->tsz;
+    // Budget split, bytes per cell: state x2, gradients, iv, slots; ~1.75 face entries per
+    // cell (records + metadata) and ~0.6 halo ids per cell, as the wedge meshes need.
+    const double per_cell = 2 * 4 * ts + 8 * ts + ts + A->Wp * 2 + 1.75 * (8 * ts + 16) + 0.6 * 4;
+    size_t budget = p.hbm_budget;
+    size_t C = (size_t) (budget / per_cell);
+    C = std::min<size_t>(C, (size_t) 1 << 30);   // cell indices stay within int
+    C = (C / A->B) * A->B;
+    if (C < (size_t) A->B) return fail(HCFD_EINVAL, "arena_create: budget below one tile");
+    A->Ccap = C;
+    A->Ecap = (size_t) (1.75 * C) / 4 * 4;
+    A->HLcap = (size_t) (0.6 * C);
+    A->tiles_cap = C / A->B;
+    A->fc.init(C / A->B);
+    A->fe.init(A->Ecap / 4);
+    A->fh.init(A->HLcap);
+    A->inst.resize(p.max_instances);
+    CK(cudaStreamCreateWithFlags(&A->stream, cudaStreamNonBlocking));
+    hcfd_arena* h = A.get();
+    auto bail = [&](int code) { arena_free(h); A.release(); delete h; return code; };
+    int rc;
+    if ((rc = dalloc((char**) &h->U[0], 4 * ts * C)) || (rc = dalloc((char**) &h->U[1], 4 * ts * C)) ||
+        (rc = dalloc((char**) &h->phiG, 8 * ts * C)) || (rc = dalloc((char**) &h->iv, ts * C)) ||
+        (rc = dalloc(&h->cslot, h->Wp * C)) || (rc = dalloc((char**) &h->tgeo, 8 * ts * h->Ecap)) ||
+        (rc = dalloc(&h->tmeta, 8 * h->Ecap)) || (rc = dalloc(&h->halo, h->HLcap)) ||
+        (rc = dalloc(&h->inst_dt, p.max_instances)) || (rc = dalloc(&h->inst_dtmin, 2 * (size_t) p.max_instances)) ||
+        (rc = dalloc(&h->inst_bc, p.max_instances)) || (rc = dalloc(&h->stats, p.max_instances)) ||
+        (rc = dalloc(&h->tiles, 2 * h->tiles_cap)) || (rc = dalloc(&h->act, p.max_instances)) ||
+        (rc = dalloc(&h->tile_r2, h->tiles_cap)) || (rc = dalloc(&h->tile_bad, h->tiles_cap)) || (rc = dalloc(&h->err, 1)))
+        return bail(rc);
+    cudaError_t ce = cudaMemsetAsync(h->err, 0, sizeof(unsigned int), h->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->U[0], 0, 4 * ts * C, h->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->U[1], 0, 4 * ts * C, h->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->phiG, 0, 8 * ts * C, h->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->iv, 0, ts * C, h->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+    if (ce != cudaSuccess) return bail(fail(HCFD_ECUDA, std::string("arena_create: ") + cudaGetErrorString(ce)));
+    rc = h->fp32() ? (h->W == 3 ? setup_kernels<float, 3>(h) : setup_kernels<float, 4>(h))
+                   : (h->W == 3 ? setup_kernels<double, 3>(h) : setup_kernels<double, 4>(h));
+    if (rc) return bail(rc);
+    *out = A.release();
+    return HCFD_OK;
+}
+
+int hcfd_arena_admit(hcfd_arena* A, const hcfd_mesh_view* mv, const int* bcmap, int nbcmap, const double* qbc,
+                     const double* qic, double dt_or_cfl, int* slot_out) {
+    hcfd::clear_error();
+    if (!A || !mv || !bcmap || !qbc || !qic || !slot_out || !(dt_or_cfl > 0)) return fail(HCFD_EINVAL, "arena_admit: bad argument");
+    CK(cudaSetDevice(A->device));
+    int rc = hcfd::validate_view(*mv);
+    if (rc) return rc;
+    int slot = -1;
+    for (size_t k = 0; k < A->inst.size(); k++) if (!A->inst[k].active) { slot = (int) k; break; }
+    if (slot < 0) return fail(HCFD_EAGAIN, "arena_admit: all instance slots in use");
+    const int Nc = mv->Nc, Nf = mv->Nf, Ncol = mv->Ncol, NBC = mv->NBCcol;
+    if (NBC > hcfd::MAXBC) return fail(HCFD_EINVAL, "arena_admit: more than 16 boundary colours");
+    const int F_BC = mv->coloff[Ncol - NBC];
+    std::vector<int> cf_off, cf_con;
+    hcfd::build_cf(Nc, Nf, mv->fc_con, cf_off, cf_con);
+    std::vector<char> ghost(Nc, 0);
+    for (int f = F_BC; f < Nf; f++) ghost[mv->fc_con[2 * f + 1]] = 1;
+    int nreal = 0, maxdeg = 0;
+    for (int c = 0; c < Nc; c++) if (!ghost[c]) { nreal++; maxdeg = std::max(maxdeg, cf_off[c + 1] - cf_off[c]); }
+    if (maxdeg > A->W) return fail(HCFD_EINVAL, "arena_admit: cells with more faces than the arena's slots");
+    std::vector<int> perm = hcfd::morton_order(*mv);
+    std::vector<int> bc_first;
+    for (int col = Ncol - NBC; col < Ncol; col++) bc_first.push_back(mv->coloff[col]);
+    hcfd::TilePlan P;
+    rc = hcfd::build_tile_plan(*mv, cf_off, cf_con, ghost, perm, F_BC, bc_first, A->B, A->W, P);
+    if (rc) return rc;
+    if (P.Hmax > A->Hcap || P.Fmax > A->Fcap) return fail(HCFD_EINVAL, "arena_admit: a tile's halo or faces exceed the arena's staging capacity");
+    // BC table (Euler::gather_BCs, src/Base/Euler.cpp:42-60)
+    hcfd::BCTable bc{};
+    bc.nbc = NBC;
+    for (int col = Ncol - NBC; col < Ncol; col++) {
+        const int b = col - (Ncol - NBC), tag = mv->coltag[col];
+        if (tag < 0 || tag >= nbcmap || bcmap[tag] < HCFD_SYMMETRY || bcmap[tag] > HCFD_SUBOUTLET)
+            return fail(HCFD_EINVAL, "arena_admit: bad BC map");
+        bc.type[b] = bcmap[tag];
+        bc.F1[b] = mv->coloff[col];
+        for (int v = 0; v < 4; v++) bc.QBC[b][v] = qbc[4 * b + v];
+        prim_to_cons(bc.QBC[b], A->prm.gma, bc.UBC[b]);
+    }
+    bc.F1[NBC] = Nf;
+    // ranges in the arena (budget admission)
+    Inst I;
+    I.Nc = Nc; I.Nf = Nf; I.Nreal = nreal; I.ntiles = P.ntiles;
+    I.ncell = (size_t) P.ntiles * A->B;
+    I.ne = P.efid.size();
+    I.nh = P.halo.size();
+    size_t ct = 0, eo = 0, ho = 0;
+    if (!A->fc.alloc(P.ntiles, ct)) return fail(HCFD_EAGAIN, "arena_admit: cell capacity exhausted");
+    if (!A->fe.alloc(I.ne / 4, eo)) { A->fc.release(ct, P.ntiles); return fail(HCFD_EAGAIN, "arena_admit: face capacity exhausted"); }
+    if (!A->fh.alloc(I.nh, ho)) {
+        A->fc.release(ct, P.ntiles); A->fe.release(eo, I.ne / 4);
+        return fail(HCFD_EAGAIN, "arena_admit: halo capacity exhausted");
+    }
+    I.c0 = ct * A->B; I.e0 = eo * 4; I.h0 = ho;
+    auto undo = [&]() { A->fc.release(ct, P.ntiles); A->fe.release(eo, I.ne / 4); A->fh.release(ho, I.nh); };
+    // tile descriptors with arena offsets
+    I.tiles.resize(8 * (size_t) P.ntiles);
+    for (int t = 0; t < P.ntiles; t++) {
+        int* d = &I.tiles[8 * (size_t) t];
+        d[0] = (int) (I.c0 + (size_t) t * A->B);
+        d[1] = (int) (I.e0 + P.foff[t]);
+        d[2] = P.foff[t + 1] - P.foff[t];
+        d[3] = slot;
+        d[4] = (int) (I.h0 + P.hoff[t]);
+        d[5] = P.hoff[t + 1] - P.hoff[t];
+        d[6] = d[7] = 0;
+    }
+    std::vector<int> halo_g(P.halo.size());
+    for (size_t k = 0; k < P.halo.size(); k++) halo_g[k] = (int) (I.c0 + P.halo[k]);
+    std::vector<int> iperm(Nc);
+    for (int i = 0; i < Nc; i++) iperm[perm[i]] = i;
+    std::vector<int> fc_g(2 * (size_t) Nf);
+    for (size_t k = 0; k < fc_g.size(); k++) fc_g[k] = (int) (I.c0 + iperm[mv->fc_con[k]]);
+    std::vector<int> foff_rel(P.foff);
+    // device work: geometry of this mesh (temporaries), then the arena ranges
+    cudaStream_t st = A->stream;
+    int *d_fn = nullptr, *d_fcu = nullptr, *d_fcg = nullptr, *d_cnoff = nullptr, *d_cncon = nullptr, *d_cfoff = nullptr,
+        *d_cfcon = nullptr, *d_efid = nullptr, *d_foff = nullptr;
+    double *d_nodes = nullptr, *d_xc = nullptr, *d_ivu = nullptr;
+    hcfd::FaceGeo<double>* d_geo = nullptr;
+    const int ncn = mv->cn_off[Nc];
+    auto tmp_free = [&]() {
+        cudaStreamSynchronize(st);
+        void* t[] = {d_fn, d_fcu, d_fcg, d_cnoff, d_cncon, d_cfoff, d_cfcon, d_efid, d_foff, d_nodes, d_xc, d_ivu, d_geo};
+        for (void* q : t) if (q) cudaFree(q);
+    };
+    if ((rc = dalloc(&d_fn, 2 * (size_t) Nf)) || (rc = dalloc(&d_fcu, 2 * (size_t) Nf)) || (rc = dalloc(&d_fcg, 2 * (size_t) Nf)) ||
+        (rc = dalloc(&d_cnoff, Nc + 1)) || (rc = dalloc(&d_cncon, ncn)) || (rc = dalloc(&d_cfoff, Nc + 1)) ||
+        (rc = dalloc(&d_cfcon, cf_con.size())) || (rc = dalloc(&d_efid, I.ne)) || (rc = dalloc(&d_foff, foff_rel.size())) ||
+        (rc = dalloc(&d_nodes, 2 * (size_t) mv->Nn)) || (rc = dalloc(&d_xc, 2 * (size_t) Nc)) || (rc = dalloc(&d_ivu, Nc)) ||
+        (rc = dalloc(&d_geo, Nf)) || (rc = dalloc(&I.d_perm, Nc))) {
+        tmp_free();
+        if (I.d_perm) cudaFree(I.d_perm);
+        undo();
+        return rc;
+    }
+    cudaError_t ce = cudaSuccess;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (ce == cudaSuccess && bytes) ce = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    };
+    up(d_fn, mv->fn_con, 8 * (size_t) Nf);
+    up(d_fcu, mv->fc_con, 8 * (size_t) Nf);
+    up(d_fcg, fc_g.data(), 4 * fc_g.size());
+    up(d_cnoff, mv->cn_off, 4 * (size_t) (Nc + 1));
+    up(d_cncon, mv->cn_con, 4 * (size_t) ncn);
+    up(d_cfoff, cf_off.data(), 4 * cf_off.size());
+    up(d_cfcon, cf_con.data(), 4 * cf_con.size());
+    up(d_efid, P.efid.data(), 4 * I.ne);
+    up(d_foff, foff_rel.data(), 4 * foff_rel.size());
+    up(d_nodes, mv->nodes, 16 * (size_t) mv->Nn);
+    up(I.d_perm, perm.data(), 4 * (size_t) Nc);
+    up(A->tmeta + 8 * I.e0, P.meta.data(), 2 * P.meta.size());
+    up(A->cslot + A->Wp * I.c0, P.cslot.data(), 2 * P.cslot.size());
+    up(A->halo + I.h0, halo_g.data(), 4 * halo_g.size());
+    const double inf2[2] = {0, 0};
+    (void) inf2;
+    if (ce == cudaSuccess) {
+        hcfd::geom_xc_kernel<<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_cnoff, d_cncon, d_nodes, d_xc);
+        hcfd::geom_face_kernel<<<nblk(Nf, 256), 256, 0, st>>>(Nf, F_BC, d_fn, d_fcu, d_nodes, d_xc, d_geo);
+        hcfd::geom_iv_kernel<<<nblk(Nc, 256), 256, 0, st>>>(Nc, F_BC, d_cfoff, d_cfcon, d_fcu, d_geo, d_ivu);
+        ce = cudaMemsetAsync((char*) A->iv + A->tsz * I.c0, 0, A->tsz * I.ncell, st);
+        if (A->fp32()) {
+            arena_iv_kernel<float><<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_ivu, I.d_perm, (float*) A->iv + I.c0);
+            hcfd::gather_geo_kernel<float><<<P.ntiles, 128, 0, st>>>(P.ntiles, d_foff, d_efid, d_geo, (float*) A->tgeo + 8 * I.e0);
+        } else {
+            arena_iv_kernel<double><<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_ivu, I.d_perm, (double*) A->iv + I.c0);
+            hcfd::gather_geo_kernel<double><<<P.ntiles, 128, 0, st>>>(P.ntiles, d_foff, d_efid, d_geo, (double*) A->tgeo + 8 * I.e0);
+        }
+        // initial state (Euler::initialise, src/Base/Euler.cpp:62-77) into the current buffer
+        double u[4];
+        prim_to_cons(qic, A->prm.gma, u);
+        const int nfill = (int) I.ncell;
+        if (A->fp32()) {
+            arena_fill_kernel<float><<<nblk(nfill, 256), 256, 0, st>>>(A->Ccap, I.c0, nfill, (Cell4<float>*) A->U[A->cur], u[0], u[1], u[2], u[3]);
+            if (Nf > F_BC)
+                hcfd::bc_cells_kernel<float><<<nblk(Nf - F_BC, 256), 256, 0, st>>>((int) A->Ccap, Nf, F_BC, d_fcg, d_geo,
+                                                                                   (Cell4<float>*) A->U[A->cur], float(A->prm.gma), bc);
+        } else {
+            arena_fill_kernel<double><<<nblk(nfill, 256), 256, 0, st>>>(A->Ccap, I.c0, nfill, (Cell4<double>*) A->U[A->cur], u[0], u[1], u[2], u[3]);
+            if (Nf > F_BC)
+                hcfd::bc_cells_kernel<double><<<nblk(Nf - F_BC, 256), 256, 0, st>>>((int) A->Ccap, Nf, F_BC, d_fcg, d_geo,
+                                                                                    (Cell4<double>*) A->U[A->cur], A->prm.gma, bc);
+        }
+        if (ce == cudaSuccess) ce = cudaGetLastError();
+    }
+    const unsigned long long infb[2] = {0x7FF0000000000000ULL, 0x7FF0000000000000ULL};
+    up(A->inst_dtmin + 2 * slot, infb, sizeof(infb));
+    up(A->inst_dt + slot, &dt_or_cfl, sizeof(double));
+    up(A->inst_bc + slot, &bc, sizeof(bc));
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(A->stats + slot, 0, sizeof(hcfd::StepStats), st);
+    tmp_free();
+    if (ce != cudaSuccess) {
+        cudaFree(I.d_perm);
+        undo();
+        return fail(HCFD_ECUDA, std::string("arena_admit: ") + cudaGetErrorString(ce));
+    }
+    I.dt = dt_or_cfl;
+    I.active = true;
+    I.admitted_step = A->steps_done;
+    A->inst[slot] = std::move(I);
+    rc = rebuild_active(A);
+    if (rc) return rc;
+    *slot_out = slot;
+    return HCFD_OK;
+}
+
+int hcfd_arena_step(hcfd_arena* A, int nsteps) {
+    hcfd::clear_error();
+    if (!A || nsteps < 0) return fail(HCFD_EINVAL, "arena_step: bad argument");
+    CK(cudaSetDevice(A->device));
+    if (A->nact == 0 || nsteps == 0) return HCFD_OK;
+    // one graph holds two steps (the ping-pong buffers and dt slots return to their start)
+    if (!A->graph) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(A->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = HCFD_OK;
+        for (int k = 0; k < 2 && rc == HCFD_OK; k++)
+            rc = A->fp32() ? enqueue_step_w<float>(A, A->cur ^ k, A->par ^ k) : enqueue_step_w<double>(A, A->cur ^ k, A->par ^ k);
+        cudaError_t e = cudaStreamEndCapture(A->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("arena_step: capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&A->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("arena_step: instantiate: ") + cudaGetErrorString(e));
+        A->graph_steps = 2;
+    }
+    int n = nsteps;
+    while (n >= 2) {
+        CK(cudaGraphLaunch(A->graph, A->stream));
+        n -= 2;
+    }
+    if (n == 1) {
+        int rc = A->fp32() ? enqueue_step_w<float>(A, A->cur, A->par) : enqueue_step_w<double>(A, A->cur, A->par);
+        if (rc) return rc;
+        A->cur ^= 1;
+        A->par ^= 1;
+        free_graph(A);   // the graph was captured for the other parity
+    }
+    A->steps_done += nsteps;
+    return HCFD_OK;
+}
+
+int hcfd_arena_poll(hcfd_arena* A, int max, int* slots, hcfd_step_stats* stats, int* n) {
+    hcfd::clear_error();
+    if (!A || !n || max < 0 || (max > 0 && (!slots || !stats))) return fail(HCFD_EINVAL, "arena_poll: bad argument");
+    CK(cudaSetDevice(A->device));
+    std::vector<hcfd::StepStats> st(A->inst.size());
+    unsigned int err = 0;
+    CK(cudaMemcpyAsync(st.data(), A->stats, sizeof(hcfd::StepStats) * st.size(), cudaMemcpyDeviceToHost, A->stream));
+    CK(cudaMemcpyAsync(&err, A->err, sizeof(err), cudaMemcpyDeviceToHost, A->stream));
+    CK(cudaStreamSynchronize(A->stream));
+    int k = 0;
+    for (size_t i = 0; i < A->inst.size() && k < max; i++) {
+        const Inst& I = A->inst[i];
+        if (!I.active) continue;
+        slots[k] = (int) i;
+        stats[k].dt = st[i].dt_last;
+        stats[k].res_l2 = I.Nreal ? std::sqrt(st[i].res2_last / I.Nreal) : 0.0;
+        stats[k].res_first = I.Nreal ? std::sqrt(st[i].res2_first / I.Nreal) : 0.0;
+        stats[k].steps = st[i].steps;
+        stats[k].nonfinite = st[i].nonfinite;
+        k++;
+    }
+    *n = k;
+    if (err) return fail(HCFD_ETIMEOUT, "arena: a bounded device wait gave up");
+    return HCFD_OK;
+}
+
+int hcfd_arena_fetch(hcfd_arena* A, int slot, int prims, double* const* out) {
+    hcfd::clear_error();
+    if (!A || slot < 0 || slot >= (int) A->inst.size() || !A->inst[slot].active || !out)
+        return fail(HCFD_EINVAL, "arena_fetch: bad argument");
+    CK(cudaSetDevice(A->device));
+    const Inst& I = A->inst[slot];
+    double* d_out = nullptr;
+    CK(cudaMallocAsync((void**) &d_out, sizeof(double) * 4 * (size_t) I.Nc, A->stream));
+    if (A->fp32())
+        arena_out_kernel<float><<<nblk(I.Nc, 256), 256, 0, A->stream>>>(A->Ccap, I.c0, I.Nc, (const Cell4<float>*) A->U[A->cur], I.d_perm, A->prm.gma, prims, d_out);
+    else
+        arena_out_kernel<double><<<nblk(I.Nc, 256), 256, 0, A->stream>>>(A->Ccap, I.c0, I.Nc, (const Cell4<double>*) A->U[A->cur], I.d_perm, A->prm.gma, prims, d_out);
+    cudaError_t e = cudaGetLastError();
+    for (int v = 0; v < 4 && e == cudaSuccess; v++)
+        e = cudaMemcpyAsync(out[v], d_out + (size_t) v * I.Nc, sizeof(double) * I.Nc, cudaMemcpyDeviceToHost, A->stream);
+    cudaFreeAsync(d_out, A->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+    if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("arena_fetch: ") + cudaGetErrorString(e));
+    return HCFD_OK;
+}
+
+int hcfd_arena_release(hcfd_arena* A, int slot) {
+    hcfd::clear_error();
+    if (!A || slot < 0 || slot >= (int) A->inst.size() || !A->inst[slot].active) return fail(HCFD_EINVAL, "arena_release: bad slot");
+    CK(cudaSetDevice(A->device));
+    CK(cudaStreamSynchronize(A->stream));
+    Inst& I = A->inst[slot];
+    A->fc.release(I.c0 / A->B, I.ntiles);
+    A->fe.release(I.e0 / 4, I.ne / 4);
+    A->fh.release(I.h0, I.nh);
+    if (I.d_perm) cudaFree(I.d_perm);
+    I = Inst();
+    return rebuild_active(A);
+}
+
+int hcfd_arena_info(hcfd_arena* A, hcfd_arena_info_t* info) {
+    if (!A || !info) return fail(HCFD_EINVAL, "arena_info: bad argument");
+    info->cell_capacity = A->Ccap;
+    info->cells_used = A->fc.used * A->B;
+    info->face_capacity = A->Ecap;
+    info->faces_used = A->fe.used * 4;
+    info->active = A->nact;
+    info->active_tiles = A->nact_tiles;
+    info->steps = A->steps_done;
+    info->tile = A->B;
+    return HCFD_OK;
+}
+
+void hcfd_arena_destroy(hcfd_arena* A) {
+    if (!A) return;
+    arena_free(A);
+    delete A;
+}
+
+}  // extern "C"

@@ -154,6 +154,14 @@ hcfd::TileArgs<T> tile_args(hcfd_solver* s, int time_mode, double dt_or_cfl) {
     a.Hmax = s->plan.Hmax;
     a.Fmax = s->plan.Fmax;
     a.err = s->d_err;
+    a.ps = s->Nc;
+    a.tiles = nullptr;
+    a.inst_dt = nullptr;
+    a.inst_dtmin = nullptr;
+    a.inst_bc = nullptr;
+    a.tile_r2 = nullptr;
+    a.tile_bad = nullptr;
+    a.par = 0;
     return a;
 }
 
@@ -183,10 +191,10 @@ int launch_step(hcfd_solver* s, int time_mode, double dt_or_cfl) {
     if (s->tiled) {
         hcfd::TileArgs<T> a = tile_args<T>(s, time_mode, dt_or_cfl);
         if ((rc = prof_begin(s, e1))) return rc;
-        hcfd::tile_pass1_kernel<T, W><<<s->grid1, s->block + 32, s->smem1, s->stream>>>(a);
+        hcfd::tile_pass1_kernel<T, W, false><<<s->grid1, s->block + 32, s->smem1, s->stream>>>(a);
         if ((rc = prof_end(s, e1, s->ev1))) return rc;
         if ((rc = prof_begin(s, e2))) return rc;
-        hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value><<<s->grid2, s->block + 32, s->smem2, s->stream>>>(a);
+        hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value, false><<<s->grid2, s->block + 32, s->smem2, s->stream>>>(a);
         if ((rc = prof_end(s, e2, s->ev2))) return rc;
     } else {
         const int grid = nblk(s->Nc, s->block);
@@ -221,13 +229,13 @@ int setup_tiled_w(hcfd_solver* s) {
     int maxsm = 0;
     CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
     if ((int) s->smem2 > maxsm || (int) s->smem1 > maxsm) return fail(HCFD_EINVAL, "tile does not fit in shared memory");
-    CK(cudaFuncSetAttribute(hcfd::tile_pass1_kernel<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) s->smem1));
-    CK(cudaFuncSetAttribute(hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value>,
+    CK(cudaFuncSetAttribute(hcfd::tile_pass1_kernel<T, W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) s->smem1));
+    CK(cudaFuncSetAttribute(hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value, false>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int) s->smem2));
     int b1 = 0, b2 = 0;
     // blocks of the tiled kernels: `block` compute threads + one producer warp
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, hcfd::tile_pass1_kernel<T, W>, s->block + 32, s->smem1));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value>,
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, hcfd::tile_pass1_kernel<T, W, false>, s->block + 32, s->smem1));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value, false>,
                                                      s->block + 32, s->smem2));
     if (b1 < 1 || b2 < 1) return fail(HCFD_EINVAL, "tiled kernels cannot be resident");
     s->grid1 = std::min(P.ntiles, b1 * s->nsm);

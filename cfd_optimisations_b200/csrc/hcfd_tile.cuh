@@ -27,7 +27,33 @@ struct TileArgs {
     const short* __restrict__ cslot;       // [ntiles * B * Wp]: (entry << 1) | cell-is-right, or -1
     int ntiles, B, Wp, Hmax, Fmax;
     unsigned int* err;                     // bit 0: a bounded wait gave up
+    int ps;                                // plane stride of the cell planes (Nc, or the arena's capacity)
+    // Arena mode (many meshes in one flat arena; see hcfd_arena.cu).  Tile i of the active
+    // list is described by tiles[2i] = {first cell, first entry, entries, instance} and
+    // tiles[2i+1] = {first halo id, halo count, -, -}; every arena tile holds B cells.
+    const int4* __restrict__ tiles;
+    const double* __restrict__ inst_dt;    // per instance: dt (fixed mode) or CFL number
+    unsigned long long* inst_dtmin;        // per instance, two parity slots (double bits)
+    const BCTable* __restrict__ inst_bc;   // per instance
+    double* tile_r2;                       // per active tile: sum of R_rho^2 of its cells
+    int* tile_bad;                         // per active tile: a NaN/Inf appeared
+    int par;                               // which dtmin slot this step uses
 };
+
+// Cells, face entries and halo of tile t (single mesh) or of active tile t (arena).
+template <bool ARENA, class T>
+__device__ __forceinline__ void tile_info(const TileArgs<T>& a, int t, int& base, int& nb, int& f0, int& nf,
+                                          int& h0, int& nh, int& inst) {
+    if constexpr (ARENA) {
+        const int4 d0 = __ldg(a.tiles + 2 * t), d1 = __ldg(a.tiles + 2 * t + 1);
+        base = d0.x; nb = a.B; f0 = d0.y; nf = d0.z; inst = d0.w; h0 = d1.x; nh = d1.y;
+    } else {
+        base = t * a.B; nb = min(a.B, a.s.Nc - base);
+        f0 = __ldg(a.foff + t); nf = __ldg(a.foff + t + 1) - f0;
+        h0 = __ldg(a.hoff + t); nh = __ldg(a.hoff + t + 1) - h0;
+        inst = 0;
+    }
+}
 
 // ---------------------------------------------------------------------------------------
 // PTX helpers (sm_90+ bulk copies and mbarriers; sm_80+ cp.async)
@@ -144,7 +170,7 @@ __device__ __forceinline__ void compute_sync(int nthreads) {
 // cp.async and signals their completion on the same mbarrier.  The `full` barrier therefore
 // completes when all of the tile's data has landed: 1 expect-tx arrival + 32 cp.async
 // arrivals + the transaction bytes.
-template <class T, bool PASS2>
+template <class T, bool PASS2, bool ARENA>
 __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned char* smem, unsigned long long* full,
                                               unsigned long long* empty, const TileSmem<T>& L) {
     const int lane = threadIdx.x & 31;
@@ -155,9 +181,8 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
         const int buf = iter & 1;
         if (iter >= 2) mbar_wait(empty + buf, ((iter >> 1) - 1) & 1, a.err);
         unsigned char* st = smem + 128 + buf * L.stage;
-        const int base = t * a.B, nb = min(a.B, a.s.Nc - base);
-        const int f0 = __ldg(a.foff + t), nf = __ldg(a.foff + t + 1) - f0;
-        const int h0 = __ldg(a.hoff + t), nh = __ldg(a.hoff + t + 1) - h0;
+        int base, nb, f0, nf, h0, nh, inst;
+        tile_info<ARENA>(a, t, base, nb, f0, nf, h0, nh, inst);
         Cell4<T>* sU = reinterpret_cast<Cell4<T>*>(st + L.u);
         Grad8<T>* sG = reinterpret_cast<Grad8<T>*>(st + L.g);
         if (lane == 0) {
@@ -172,19 +197,19 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
 #pragma unroll
             for (int j = 0; j < CU; j++)
                 bulk_g2s(reinterpret_cast<char*>(sU) + (size_t) 16 * j * NL,
-                         reinterpret_cast<const char*>(a.s.U) + 16 * ((size_t) j * a.s.Nc + base), nb * 16u, full + buf);
+                         reinterpret_cast<const char*>(a.s.U) + 16 * ((size_t) j * a.ps + base), nb * 16u, full + buf);
             if (PASS2) {
 #pragma unroll
                 for (int j = 0; j < CG; j++)
                     bulk_g2s(reinterpret_cast<char*>(sG) + (size_t) 16 * j * NL,
-                             reinterpret_cast<const char*>(a.s.phiG) + 16 * ((size_t) j * a.s.Nc + base), nb * 16u,
+                             reinterpret_cast<const char*>(a.s.phiG) + 16 * ((size_t) j * a.ps + base), nb * 16u,
                              full + buf);
             }
             if (bf) {
                 bulk_g2s(st + L.geo, a.tgeo + (size_t) f0 * 8, bf, full + buf);
                 bulk_g2s(st + L.meta, a.tmeta + (size_t) f0 * 8, bm, full + buf);
             }
-            bulk_g2s(st + L.cslot, a.cslot + (size_t) t * a.B * a.Wp, bs, full + buf);
+            bulk_g2s(st + L.cslot, a.cslot + (size_t) base * a.Wp, bs, full + buf);
             bulk_g2s(st + L.iv, a.s.iv + base, bi, full + buf);
         }
         for (int h = lane; h < nh; h += 32) {
@@ -192,11 +217,11 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
 #pragma unroll
             for (int j = 0; j < CU; j++)
                 cp_async16(reinterpret_cast<char*>(sU) + 16 * ((size_t) j * NL + a.B + h),
-                           reinterpret_cast<const char*>(a.s.U) + 16 * ((size_t) j * a.s.Nc + ci));
+                           reinterpret_cast<const char*>(a.s.U) + 16 * ((size_t) j * a.ps + ci));
 #pragma unroll
             for (int j = 0; j < CG; j++)
                 cp_async16(reinterpret_cast<char*>(sG) + 16 * ((size_t) j * NL + a.B + h),
-                           reinterpret_cast<const char*>(a.s.phiG) + 16 * ((size_t) j * a.s.Nc + ci));
+                           reinterpret_cast<const char*>(a.s.phiG) + 16 * ((size_t) j * a.ps + ci));
         }
         cp_async_arrive_noinc(full + buf);
     }
@@ -322,7 +347,7 @@ struct FaceIn {
 // (producer_loop); the first NT = blockDim.x - 32 threads compute.  Compute iteration i
 // reads staging buffer i & 1 once its `full` barrier completes and releases it on its
 // `empty` barrier (one arrival per compute warp) when done.
-#define HCFD_TILE_LOOP_BEGIN(PASS2)                                                              \
+#define HCFD_TILE_LOOP_BEGIN(PASS2, ARENA)                                                       \
     const int NT = blockDim.x - 32;                                                              \
     const int NL = a.B + a.Hmax;                                                                 \
     unsigned long long* full = reinterpret_cast<unsigned long long*>(smem);                      \
@@ -334,14 +359,15 @@ struct FaceIn {
     }                                                                                            \
     __syncthreads();                                                                             \
     if ((int) threadIdx.x >= NT) {                                                               \
-        producer_loop<T, PASS2>(a, smem, full, empty, L);                                        \
+        producer_loop<T, PASS2, ARENA>(a, smem, full, empty, L);                                 \
     } else {                                                                                     \
     unsigned iter = 0;                                                                           \
     for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {                             \
         const int buf = iter & 1;                                                                \
         unsigned char* st = smem + 128 + buf * L.stage;                                          \
         mbar_wait(full + buf, (iter >> 1) & 1, a.err);                                           \
-        const int base = t * a.B, nb = min(a.B, s.Nc - base);                                    \
+        int base, nb, f0t, nft, h0t, nht, inst;                                                  \
+        tile_info<ARENA>(a, t, base, nb, f0t, nft, h0t, nht, inst);                              \
         const Cell4<T>* sU = reinterpret_cast<const Cell4<T>*>(st + L.u);                        \
         const T* sGeo = reinterpret_cast<const T*>(st + L.geo);                                  \
         const int nfl = reinterpret_cast<const int*>(smem + 64)[buf];                            \
@@ -355,13 +381,13 @@ struct FaceIn {
     }                                                                                            \
     }
 
-template <class T, int W>
+template <class T, int W, bool ARENA>
 __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const TileSmem<T> L(a.B, a.Hmax, a.Fmax, W, a.Wp, false);
     const StepArgs<T>& s = a.s;
     double dtc = 1e300;
-    HCFD_TILE_LOOP_BEGIN(false)
+    HCFD_TILE_LOOP_BEGIN(false, ARENA)
     for (int c = threadIdx.x; c < nb; c += NT) {
         short cs[8];
         lds_slots(sSlot + c * a.Wp, a.Wp, cs);
@@ -428,11 +454,20 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
             out[2 * v] = phi * gx;
             out[2 * v + 1] = phi * gy;
         }
-        st_grad(s.phiG, s.Nc, base + c, out);
+        st_grad(s.phiG, a.ps, base + c, out);
         if (s.time_mode != TM_FIXED) dtc = fmin(dtc, (double) (T(1) / (iv * lam)));
     }
+    if constexpr (ARENA) {
+        // per-instance minimum: one atomic per warp and tile (min is exact, order-free)
+        if (s.time_mode != TM_FIXED) {
+            const double m = warp_min(dtc);
+            if ((threadIdx.x & 31) == 0 && m < 1e300)
+                atomicMin(a.inst_dtmin + 2 * inst + a.par, (unsigned long long) __double_as_longlong(m));
+            dtc = 1e300;
+        }
+    }
     HCFD_TILE_LOOP_END
-    if (s.time_mode != TM_FIXED) {
+    if (!ARENA && s.time_mode != TM_FIXED) {
         __shared__ double sm[32];
         double m = warp_min(dtc);
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -446,18 +481,26 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
     }
 }
 
-template <class T, int W, bool COMP>
+template <class T, int W, bool COMP, bool ARENA>
 __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const TileSmem<T> L(a.B, a.Hmax, a.Fmax, W, a.Wp, true);
     const StepArgs<T>& s = a.s;
     T* sF = reinterpret_cast<T*>(smem + L.flux);     // [5][B * W]: Af, F0..F3
     const int BW = a.B * W;
-    const double dt_used = (s.time_mode == TM_FIXED) ? s.dt_or_cfl
-                                                      : s.dt_or_cfl * __longlong_as_double((long long) *s.dtmin);
+    double dt_used = (s.time_mode == TM_FIXED) ? s.dt_or_cfl
+                                                : s.dt_or_cfl * __longlong_as_double((long long) *s.dtmin);
     double r2 = 0.0;
     int bad = 0;
-    HCFD_TILE_LOOP_BEGIN(true)
+    __shared__ double s_wr2[8];
+    __shared__ int s_wbad[8];
+    HCFD_TILE_LOOP_BEGIN(true, ARENA)
+    T cfl_or_dt = T(s.dt_or_cfl);
+    if constexpr (ARENA) {
+        const double v = __ldg(a.inst_dt + inst);
+        cfl_or_dt = T(v);
+        dt_used = (s.time_mode == TM_FIXED) ? v : v * __longlong_as_double((long long) a.inst_dtmin[2 * inst + a.par]);
+    }
     const Grad8<T>* sG = reinterpret_cast<const Grad8<T>*>(st + L.g);
     const int nf = nfl;
     // face phase: one Rusanov flux per face entry (Flux.cpp:19-38).  Each thread takes two
@@ -512,7 +555,7 @@ __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
             }
         }
         T dt;
-        if (s.time_mode == TM_LOCAL) dt = T(s.dt_or_cfl) * (T(1) / (iv * lam));
+        if (s.time_mode == TM_LOCAL) dt = cfl_or_dt * (T(1) / (iv * lam));
         else dt = T(dt_used);
         T un_[4];
 #pragma unroll
@@ -523,7 +566,7 @@ __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
             if (v == 0) r2 += (double) Rv * (double) Rv;
             bad |= !isfinite(un_[v]);
         }
-        st_cell(s.Unew, s.Nc, base + c, un_);
+        st_cell(s.Unew, a.ps, base + c, un_);
         // ghost refresh (Euler.cpp:96, :138-142): this cell is its ghosts' only neighbour
 #pragma unroll
         for (int k = 0; k < W; k++) {
@@ -532,17 +575,35 @@ __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
             const int bc = sMeta[8 * e + 4];
             if (bc < 0) continue;
             const int lb = sMeta[8 * e + 1];
-            const int gi = lb < a.B ? base + lb : __ldg(a.halo + a.hoff[t] + lb - a.B);
+            const int gi = lb < a.B ? base + lb : __ldg(a.halo + h0t + lb - a.B);
             FaceGeo<T> g;
             lds_geo(sGeo, nfl, e, g);
             T ug[4];
-            ghost_state(s.bc.type[bc], un_, g.nx, g.ny, s.gma, s.bc.UBC[bc], s.bc.QBC[bc], ug);
-            st_cell(s.Unew, s.Nc, gi, ug);
+            const BCTable* bt = ARENA ? a.inst_bc + inst : &s.bc;
+            ghost_state(bt->type[bc], un_, g.nx, g.ny, s.gma, bt->UBC[bc], bt->QBC[bc], ug);
+            st_cell(s.Unew, a.ps, gi, ug);
         }
     }
+    if constexpr (ARENA) {
+        // per-tile residual: warp sums, then the warps in order (deterministic)
+        const double w = warp_sum(r2);
+        const int wb = __any_sync(0xffffffffu, bad);
+        if ((threadIdx.x & 31) == 0) { s_wr2[threadIdx.x >> 5] = w; s_wbad[threadIdx.x >> 5] = wb; }
+        r2 = 0.0;
+        bad = 0;
+    }
     compute_sync(NT);   // the next tile's face phase overwrites the flux slots
+    if constexpr (ARENA) {
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            int b = 0;
+            for (int k = 0; k < NT / 32; k++) { tot += s_wr2[k]; b |= s_wbad[k]; }
+            a.tile_r2[t] = tot;
+            a.tile_bad[t] = b;
+        }
+    }
     HCFD_TILE_LOOP_END
-    finish_step(s, r2, bad, dt_used);
+    if constexpr (!ARENA) finish_step(s, r2, bad, dt_used);
 }
 
 // Face records in tile order, component-major per tile: for tile t with entries

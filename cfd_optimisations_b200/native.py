@@ -48,6 +48,18 @@ class StepStats(ct.Structure):
                 ("steps", ct.c_longlong), ("nonfinite", ct.c_int)]
 
 
+class ArenaParams(ct.Structure):
+    _fields_ = [("hbm_budget", ct.c_size_t), ("precision", ct.c_int), ("limiter", ct.c_int),
+                ("venkat_K", ct.c_double), ("gma", ct.c_double), ("time_mode", ct.c_int), ("tile", ct.c_int),
+                ("slots", ct.c_int), ("max_instances", ct.c_int)]
+
+
+class ArenaInfo(ct.Structure):
+    _fields_ = [("cell_capacity", ct.c_size_t), ("cells_used", ct.c_size_t), ("face_capacity", ct.c_size_t),
+                ("faces_used", ct.c_size_t), ("active", ct.c_int), ("active_tiles", ct.c_int),
+                ("steps", ct.c_longlong), ("tile", ct.c_int)]
+
+
 class NoallocMesh(ct.Structure):
     _fields_ = [("Nc", ct.c_int), ("Nf", ct.c_int), ("F_BC", ct.c_int), ("slots", ct.c_int),
                 ("slot", ct.c_void_p), ("geo", ct.c_void_p), ("iv", ct.c_void_p),
@@ -97,6 +109,14 @@ _SIGS = {
     "hcfd_plan_check": (ct.c_int, [ct.POINTER(MeshView), ct.c_int, ct.c_int, ct.POINTER(ct.c_longlong)]),
     "hcfd_step_noalloc": (ct.c_int, [ct.POINTER(NoallocMesh), ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_double,
                                      ct.c_void_p, _dp, _dp]),
+    "hcfd_arena_create": (ct.c_int, [ct.POINTER(ArenaParams), ct.POINTER(ct.c_void_p)]),
+    "hcfd_arena_admit": (ct.c_int, [ct.c_void_p, ct.POINTER(MeshView), _ip, ct.c_int, _dp, _dp, ct.c_double, _ip]),
+    "hcfd_arena_step": (ct.c_int, [ct.c_void_p, ct.c_int]),
+    "hcfd_arena_poll": (ct.c_int, [ct.c_void_p, ct.c_int, _ip, ct.POINTER(StepStats), _ip]),
+    "hcfd_arena_fetch": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(_dp)]),
+    "hcfd_arena_release": (ct.c_int, [ct.c_void_p, ct.c_int]),
+    "hcfd_arena_info": (ct.c_int, [ct.c_void_p, ct.POINTER(ArenaInfo)]),
+    "hcfd_arena_destroy": (None, [ct.c_void_p]),
     "hcfd_set_device": (ct.c_int, [ct.c_int, _ip]),
     "hcfd_device_sync": (ct.c_int, []),
     "hcfd_last_error": (ct.c_char_p, []),

@@ -216,6 +216,50 @@ int  hcfd_host_unpin(void* p);
  * face entries, slots per cell, total halo cells.  No reference counterpart. */
 int  hcfd_plan_check(const hcfd_mesh_view* mesh, int tile, int keep_numbering, long long* info);
 
+/* ---- batched and served solves: many meshes in one device arena --------------------- */
+
+/* No counterpart in the reference (it solves one mesh per process).  An arena packs many
+ * meshes (instances) into one flat set of device arrays sized from an HBM budget; each
+ * admitted mesh gets contiguous ranges (per-instance offsets), its own BC table, dt or CFL
+ * number and statistics, and all active instances advance together through the tiled step
+ * kernels, a chunk of steps replayed as one CUDA graph.  An instance's arithmetic does not
+ * depend on what else is in the arena: its state is the same alone and in the mix. */
+typedef struct hcfd_arena hcfd_arena;
+typedef struct hcfd_arena_params {
+    size_t hbm_budget;      /* bytes of device memory the arena's arrays may use            */
+    int    precision;       /* enum hcfd_precision                                          */
+    int    limiter;         /* enum hcfd_limiter                                            */
+    double venkat_K;
+    double gma;
+    int    time_mode;       /* enum hcfd_time_mode, shared by all instances                 */
+    int    tile;            /* cells per tile (32..256, multiple of 32), 0 = 128            */
+    int    slots;           /* faces per cell: 3 (triangles) or 4 (quads), 0 = 3            */
+    int    max_instances;   /* instance slots                                               */
+} hcfd_arena_params;
+typedef struct hcfd_arena_info_t {
+    size_t cell_capacity, cells_used, face_capacity, faces_used;
+    int active, active_tiles;
+    long long steps;
+    int tile;
+} hcfd_arena_info_t;
+
+int  hcfd_arena_create(const hcfd_arena_params* params, hcfd_arena** out);
+/* Admits one mesh with its BC map and states (as hcfd_gpu_gather_bcs), its initial state
+ * (as hcfd_gpu_initialise) and its dt (fixed mode) or CFL number.  Returns HCFD_EAGAIN when
+ * the budget, a free range or an instance slot is missing: retry after a release. */
+int  hcfd_arena_admit(hcfd_arena* a, const hcfd_mesh_view* mesh, const int* bcmap, int nbcmap, const double* qbc,
+                      const double* qic, double dt_or_cfl, int* slot);
+/* Advances every active instance by nsteps steps (enqueued; returns without waiting). */
+int  hcfd_arena_step(hcfd_arena* a, int nsteps);
+/* Waits, then reports up to max active instances: their slots and step statistics. */
+int  hcfd_arena_poll(hcfd_arena* a, int max, int* slots, hcfd_step_stats* stats, int* n);
+/* Copies one instance's state (prims != 0: primitive) to 4 host arrays of its Nc doubles. */
+int  hcfd_arena_fetch(hcfd_arena* a, int slot, int prims, double* const* out);
+/* Retires an instance and frees its ranges for later admissions. */
+int  hcfd_arena_release(hcfd_arena* a, int slot);
+int  hcfd_arena_info(hcfd_arena* a, hcfd_arena_info_t* info);
+void hcfd_arena_destroy(hcfd_arena* a);
+
 /* ---- one step without device allocation -------------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc: a framework
