@@ -15,8 +15,9 @@ class Arena:
 
     def __init__(self, hbm_budget: int, precision: int = FP32, limiter: int = LIMITER_BJ, venkat_K: float = 5.0,
                  gma: float = 1.4, time_mode: int = GLOBAL_CFL, tile: int = 0, slots: int = 3,
-                 max_instances: int = 1024):
-        p = _n.ArenaParams(int(hbm_budget), precision, limiter, venkat_K, gma, time_mode, tile, slots, max_instances)
+                 max_instances: int = 1024, freeze_limiter_after: int = 0):
+        p = _n.ArenaParams(int(hbm_budget), precision, limiter, venkat_K, gma, time_mode, tile, slots, max_instances,
+                           freeze_limiter_after)
         h = ct.c_void_p()
         _n.check(_n.lib().hcfd_arena_create(ct.byref(p), ct.byref(h)))
         self._h = h

@@ -1,0 +1,116 @@
+"""Batched solves: many wedge instances of uneven size packed into one device arena and
+advanced together, against the plain FP64 solver looped over the same instances.
+
+    python -m cfd_optimisations_b200.batched [--instances 512 --steps 2000 --seed 2024]
+
+Instances: triangle counts log-uniform in [2,000, 200,000] on a 2:1 node grid, M ~ U[1.8, 4.0],
+ramp angle ~ U[5, 15] degrees, a jitter/permutation seed per instance; freestream initial
+state; Barth-Jespersen limiter; global CFL 0.5 per instance; a fixed number of steps each.
+The arena runs in FP32 with compensated residual sums, its tile size picked by the
+autotuner (autotune.py) for the median instance size; the loop runs each instance alone
+through the plain FP64 solver.  Prints one JSON object: device throughput of both, the
+speed-up, and the FP32 arena's relative L-inf error against the FP64 loop per instance.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+
+from . import FP32, FP64, GLOBAL_CFL, LIMITER_BJ, NUMBER_RANDOM, Mesh, Solver, wedge_case
+from . import autotune
+from .arena import Arena
+
+
+def instance_specs(n: int = 512, seed: int = 2024, lo: float = 2e3, hi: float = 2e5):
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n):
+        ntri = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        ny1 = max(2, int(round(math.sqrt(ntri / 4.0))))
+        specs.append(dict(nx=2 * ny1 + 1, ny=ny1 + 1, mach=float(rng.uniform(1.8, 4.0)),
+                          theta=float(rng.uniform(5.0, 15.0)), seed=1234 + i))
+    return specs
+
+
+def build(specs):
+    return [Mesh.wedge(s["nx"], s["ny"], theta_deg=s["theta"], seed=s["seed"], numbering=NUMBER_RANDOM)
+            for s in specs]
+
+
+def run_arena(meshes, specs, steps, precision=FP32, limiter=LIMITER_BJ, cfl=0.5, tile=0):
+    cells = sum(m.Nc for m in meshes)
+    a = Arena(int(max(2e9, 400.0 * cells)), precision=precision, limiter=limiter, tile=tile,
+              max_instances=len(meshes) + 8)
+    slots = []
+    t0 = time.perf_counter()
+    for m, s in zip(meshes, specs):
+        bcmap, qbc, q = wedge_case(s["mach"])
+        k = a.admit(m, bcmap, qbc, q, cfl)
+        if k is None:
+            raise RuntimeError("arena full")
+        slots.append(k)
+    t_admit = time.perf_counter() - t0
+    a.step(2)
+    a.poll()
+    t0 = time.perf_counter()
+    a.step(steps - 2)
+    stats = a.poll()
+    t_run = time.perf_counter() - t0
+    return a, slots, stats, t_admit, t_run
+
+
+def run_loop(meshes, specs, steps, precision=FP64, limiter=LIMITER_BJ, cfl=0.5):
+    ms, t_create, out = 0.0, 0.0, []
+    for m, s in zip(meshes, specs):
+        bcmap, qbc, q = wedge_case(s["mach"])
+        t0 = time.perf_counter()
+        sol = Solver(m, precision=precision, limiter=limiter)
+        sol.gather_bcs(bcmap, qbc)
+        sol.initialise(q)
+        t_create += time.perf_counter() - t0
+        sol.step(2, GLOBAL_CFL, cfl)
+        ms += sol.step_timed(steps - 2, GLOBAL_CFL, cfl)
+        out.append(sol.U())
+        del sol
+    return ms, t_create, out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-loop", action="store_true", help="skip the FP64 loop baseline")
+    a = ap.parse_args()
+    specs = instance_specs(a.instances, a.seed)
+    t0 = time.perf_counter()
+    meshes = build(specs)
+    t_gen = time.perf_counter() - t0
+    real = [m.Nc - (2 * (s["nx"] - 1) + 2 * (s["ny"] - 1)) for m, s in zip(meshes, specs)]
+    median = int(np.median(real))
+    shape = autotune.best(median, FP32, LIMITER_BJ, arena_shapes=True)
+    arena, slots, stats, t_admit, t_run = run_arena(meshes, specs, a.steps, tile=shape["tile"])
+    upd = sum(real) * (a.steps - 2)
+    out = dict(workload=dict(instances=a.instances, steps=a.steps, triangles_total=int(sum(real)),
+                             triangles_median=median, seed=a.seed, limiter="barth-jespersen", cfl=0.5),
+               mesh_generation_s=t_gen,
+               arena=dict(precision="fp32-compensated", tile=shape["tile"], admit_s=t_admit, run_s=t_run,
+                          cell_updates_per_s=upd / t_run, solves_per_s=a.instances / t_run,
+                          nonfinite=sum(1 for s in stats.values() if s["nonfinite"])))
+    if not a.no_loop:
+        ms, t_create, U64 = run_loop(meshes, specs, a.steps)
+        errs = [float(np.max(np.abs(arena.fetch(k) - u).max(axis=1) / np.abs(u).max(axis=1)))
+                for k, u in zip(slots, U64)]
+        out["fp64_loop"] = dict(device_s=ms / 1e3, create_s=t_create, cell_updates_per_s=upd / (ms / 1e3),
+                                solves_per_s=a.instances / (ms / 1e3))
+        out["speedup_solves_per_s"] = out["arena"]["solves_per_s"] / out["fp64_loop"]["solves_per_s"]
+        out["fp32_vs_fp64_rel_linf"] = dict(max=max(errs), median=float(np.median(errs)))
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -151,6 +151,7 @@ struct hcfd_arena {
     // device arrays
     void* U[2] = {nullptr, nullptr};
     void* phiG = nullptr;
+    void* phiF = nullptr;
     void* iv = nullptr;
     short* cslot = nullptr;
     void* tgeo = nullptr;
@@ -198,6 +199,9 @@ hcfd::TileArgs<T> arena_args(hcfd_arena* A, int cur, int par) {
     s.time_mode = A->time_mode;
     s.gma = T(A->prm.gma);
     s.venkat_K = T(A->prm.venkat_K);
+    s.phiF = (Cell4<T>*) A->phiF;
+    s.freeze_after = A->prm.freeze_limiter_after;
+    a.inst_stats = A->stats;
     a.tgeo = (const T*) A->tgeo;
     a.tmeta = A->tmeta;
     a.halo = A->halo;
@@ -292,7 +296,7 @@ void arena_free(hcfd_arena* A) {
     if (A->stream) cudaStreamSynchronize(A->stream);
     free_graph(A);
     for (auto& I : A->inst) if (I.d_perm) cudaFree(I.d_perm);
-    void* p[] = {A->U[0], A->U[1], A->phiG, A->iv, A->cslot, A->tgeo, A->tmeta, A->halo, A->inst_dt, A->inst_dtmin,
+    void* p[] = {A->U[0], A->U[1], A->phiG, A->phiF, A->iv, A->cslot, A->tgeo, A->tmeta, A->halo, A->inst_dt, A->inst_dtmin,
                  A->inst_bc, A->stats, A->tiles, A->act, A->tile_r2, A->tile_bad, A->err};
     for (void* q : p) if (q) cudaFree(q);
     if (A->stream) cudaStreamDestroy(A->stream);
@@ -316,7 +320,8 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
     if (p.hbm_budget < ((size_t) 16 << 20) || !(p.gma > 1.0) || (p.precision != HCFD_FP64 && p.precision != HCFD_FP32) ||
         (p.limiter != HCFD_LIMITER_BJ && p.limiter != HCFD_LIMITER_VENKAT) || p.max_instances < 1 ||
         p.max_instances > 65536 || p.tile < 0 || p.tile > 256 || (p.tile % 32) || (p.slots != 0 && p.slots != 3 && p.slots != 4) ||
-        (p.time_mode != HCFD_FIXED_DT && p.time_mode != HCFD_GLOBAL_CFL && p.time_mode != HCFD_LOCAL_CFL))
+        (p.time_mode != HCFD_FIXED_DT && p.time_mode != HCFD_GLOBAL_CFL && p.time_mode != HCFD_LOCAL_CFL) ||
+        p.freeze_limiter_after < 0)
         return fail(HCFD_EINVAL, "arena_create: bad parameters");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(HCFD_ECUDA, "arena_create: no CUDA device");
@@ -335,7 +340,8 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
     const size_t ts = A->tsz;
     // Budget split, bytes per cell: state x2, gradients, iv, slots; ~1.75 face entries per
     // cell (records + metadata) and ~0.6 halo ids per cell, as the wedge meshes need.
-    const double per_cell = 2 * 4 * ts + 8 * ts + ts + A->Wp * 2 + 1.75 * (8 * ts + 16) + 0.6 * 4;
+    const double per_cell = 2 * 4 * ts + 8 * ts + ts + A->Wp * 2 + 1.75 * (8 * ts + 16) + 0.6 * 4 +
+                            (p.freeze_limiter_after > 0 ? 4 * ts : 0);
     size_t budget = p.hbm_budget;
     size_t C = (size_t) (budget / per_cell);
     C = std::min<size_t>(C, (size_t) 1 << 30);   // cell indices stay within int
@@ -355,6 +361,7 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
     int rc;
     if ((rc = dalloc((char**) &h->U[0], 4 * ts * C)) || (rc = dalloc((char**) &h->U[1], 4 * ts * C)) ||
         (rc = dalloc((char**) &h->phiG, 8 * ts * C)) || (rc = dalloc((char**) &h->iv, ts * C)) ||
+        (p.freeze_limiter_after > 0 && (rc = dalloc((char**) &h->phiF, 4 * ts * C))) ||
         (rc = dalloc(&h->cslot, h->Wp * C)) || (rc = dalloc((char**) &h->tgeo, 8 * ts * h->Ecap)) ||
         (rc = dalloc(&h->tmeta, 8 * h->Ecap)) || (rc = dalloc(&h->halo, h->HLcap)) ||
         (rc = dalloc(&h->inst_dt, p.max_instances)) || (rc = dalloc(&h->inst_dtmin, 2 * (size_t) p.max_instances)) ||

@@ -80,7 +80,18 @@ struct StepArgs {
     T gma, venkat_K;
     double dt_or_cfl;
     BCTable bc;
+    // Limiter freezing: the limiter values of step freeze_after are recorded in phiF and
+    // reused by every later step (freeze_after = 0: never).  Steps are counted on the device.
+    Cell4<T>* phiF;
+    long long freeze_after;
 };
+
+enum { LIM_NORMAL = 0, LIM_RECORD = 1, LIM_FROZEN = 2 };
+// How pass 1 treats the limiter in the step after `steps_before` steps.
+__device__ __forceinline__ int limiter_mode(long long steps_before, long long freeze_after) {
+    if (freeze_after <= 0 || steps_before + 1 < freeze_after) return LIM_NORMAL;
+    return steps_before + 1 == freeze_after ? LIM_RECORD : LIM_FROZEN;
+}
 
 // ---------------------------------------------------------------------------------------
 // loads
@@ -323,27 +334,35 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
                 e2 = kh * kh * kh;
             }
             const T eps = T(1e-9);
-            T out[8];
+            const int lmode = limiter_mode(a.stats->steps, a.freeze_after);
+            T out[8], phis[4];
+            if (lmode == LIM_FROZEN) ld_cell(a.phiF, a.Nc, c, phis);
 #pragma unroll
             for (int v = 0; v < 4; v++) {
                 const T gx = G[v][0] * iv, gy = G[v][1] * iv;     // GaussGreen.cpp:33-39
                 T phi = T(1);
+                if (lmode == LIM_FROZEN) {
+                    phi = phis[v];
+                } else {
 #pragma unroll
-                for (int k = 0; k < W; k++) {
-                    if (s[k].y < 0) continue;
-                    const T d = gx * ro[k][0] + gy * ro[k][1];   // Limiter.cpp:50-51
-                    T pf = T(1);
-                    if (a.limiter == LIM_BJ) {                   // Limiter.cpp:67-71
-                        // one division: the numerator is picked by the sign of d
-                        if (d > eps || d < -eps) pf = fmin(T(1), ((d > eps) ? umax[v] - u[v] : umin[v] - u[v]) / d);
-                    } else {
-                        if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
+                    for (int k = 0; k < W; k++) {
+                        if (s[k].y < 0) continue;
+                        const T d = gx * ro[k][0] + gy * ro[k][1];   // Limiter.cpp:50-51
+                        T pf = T(1);
+                        if (a.limiter == LIM_BJ) {                   // Limiter.cpp:67-71
+                            // one division: the numerator is picked by the sign of d
+                            if (d > eps || d < -eps) pf = fmin(T(1), ((d > eps) ? umax[v] - u[v] : umin[v] - u[v]) / d);
+                        } else {
+                            if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
+                        }
+                        phi = fmin(phi, pf);                         // Limiter.cpp:73-74
                     }
-                    phi = fmin(phi, pf);                         // Limiter.cpp:73-74
                 }
+                phis[v] = phi;
                 out[2 * v] = phi * gx;
                 out[2 * v + 1] = phi * gy;
             }
+            if (lmode == LIM_RECORD) st_cell(a.phiF, a.Nc, c, phis);
             st_grad(a.phiG, a.Nc, c, out);
             if (a.time_mode != TM_FIXED) dtc = (double) (T(1) / (iv * lam));
         }

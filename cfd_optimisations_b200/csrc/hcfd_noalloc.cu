@@ -127,6 +127,8 @@ extern "C" int hcfd_step_noalloc(const hcfd_noalloc_mesh* m, const double* U_in,
     a.venkat_K = m->venkat_K;
     a.dt_or_cfl = dt_or_cfl;
     a.bc = bc;
+    a.phiF = nullptr;        // no limiter freezing here
+    a.freeze_after = 0;
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     noalloc_reset_kernel<<<1, 32, 0, st>>>(a.dtmin, a.counter, a.stats);

@@ -70,6 +70,7 @@ struct hcfd_solver {
     void* d_iv = nullptr;                // T [Nc]
     void* d_U[2] = {nullptr, nullptr};   // Cell4<T> [Nc]
     void* d_phiG = nullptr;              // Grad8<T> [Nc]
+    void* d_phiF = nullptr;              // Cell4<T> [Nc]: frozen limiter values
     double* d_io = nullptr;              // 4 Nc doubles staging for upload/download
     double* d_cp = nullptr;              // Nf doubles for the wall Cp
     unsigned long long* d_dtmin = nullptr;   // [2]
@@ -107,7 +108,7 @@ void free_all(hcfd_solver* s) {
     for (auto e : s->ev1) cudaEventDestroy(e);
     for (auto e : s->ev2) cudaEventDestroy(e);
     void* ptrs[] = {s->d_fc, s->d_perm, s->d_slot, s->d_geo64, s->d_geoT, s->d_iv, s->d_U[0], s->d_U[1],
-                    s->d_phiG, s->d_io, s->d_cp, s->d_dtmin, s->d_partial, s->d_counter, s->d_err, s->d_stats,
+                    s->d_phiG, s->d_phiF, s->d_io, s->d_cp, s->d_dtmin, s->d_partial, s->d_counter, s->d_err, s->d_stats,
                     s->d_tgeo, s->d_tmeta, s->d_foff, s->d_hoff, s->d_halo, s->d_cslot};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -135,6 +136,8 @@ hcfd::StepArgs<T> step_args(hcfd_solver* s, int time_mode, double dt_or_cfl) {
     a.venkat_K = T(s->prm.venkat_K);
     a.dt_or_cfl = dt_or_cfl;
     a.bc = s->bc;
+    a.phiF = (hcfd::Cell4<T>*) s->d_phiF;
+    a.freeze_after = s->prm.freeze_limiter_after;
     return a;
 }
 
@@ -295,12 +298,12 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
     *out = nullptr;
     int rc = hcfd::validate_view(*mv);
     if (rc != HCFD_OK) return rc;
-    hcfd_params p{1.4, HCFD_LIMITER_BJ, 5.0, HCFD_FP64, 0, HCFD_KERNEL_TILED, 0, 0};
+    hcfd_params p{1.4, HCFD_LIMITER_BJ, 5.0, HCFD_FP64, 0, HCFD_KERNEL_TILED, 0, 0, 0};
     if (prm) p = *prm;
     if (!(p.gma > 1.0) || (p.limiter != HCFD_LIMITER_BJ && p.limiter != HCFD_LIMITER_VENKAT) ||
         (p.precision != HCFD_FP64 && p.precision != HCFD_FP32) || p.block < 0 || p.block > 1024 || (p.block % 32) ||
         (p.kernel != HCFD_KERNEL_TILED && p.kernel != HCFD_KERNEL_CELL) || p.tile < 0 || p.tile > 512 || (p.tile % 32) ||
-        (p.kernel == HCFD_KERNEL_TILED && p.block > 256))
+        (p.kernel == HCFD_KERNEL_TILED && p.block > 256) || p.freeze_limiter_after < 0)
         return fail(HCFD_EINVAL, "gpu_create: bad parameters");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -392,6 +395,7 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         (rc = dalloc(&h->d_geo64, Nf)) || (rc = dalloc((char**) &h->d_iv, tsz * niv)) ||
         (rc = dalloc((char**) &h->d_U[0], tsz * 4 * Nc)) || (rc = dalloc((char**) &h->d_U[1], tsz * 4 * Nc)) ||
         (rc = dalloc((char**) &h->d_phiG, tsz * 8 * Nc)) || (rc = dalloc(&h->d_io, 4 * (size_t) Nc)) ||
+        (p.freeze_limiter_after > 0 && (rc = dalloc((char**) &h->d_phiF, tsz * 4 * Nc))) ||
         (rc = dalloc(&h->d_cp, Nf)) || (rc = dalloc(&h->d_dtmin, 2)) || (rc = dalloc(&h->d_partial, h->partial_len)) ||
         (rc = dalloc(&h->d_counter, 1)) || (rc = dalloc(&h->d_err, 1)) || (rc = dalloc(&h->d_stats, 1)) ||
         (rc = dalloc(&d_fn, 2 * (size_t) Nf)) || (rc = dalloc(&d_fcu, 2 * (size_t) Nf)) ||

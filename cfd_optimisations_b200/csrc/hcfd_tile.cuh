@@ -35,6 +35,7 @@ struct TileArgs {
     const double* __restrict__ inst_dt;    // per instance: dt (fixed mode) or CFL number
     unsigned long long* inst_dtmin;        // per instance, two parity slots (double bits)
     const BCTable* __restrict__ inst_bc;   // per instance
+    const StepStats* inst_stats;           // per instance (step counts for limiter freezing)
     double* tile_r2;                       // per active tile: sum of R_rho^2 of its cells
     int* tile_bad;                         // per active tile: a NaN/Inf appeared
     int par;                               // which dtmin slot this step uses
@@ -388,6 +389,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
     const StepArgs<T>& s = a.s;
     double dtc = 1e300;
     HCFD_TILE_LOOP_BEGIN(false, ARENA)
+    const int lmode = limiter_mode(ARENA ? a.inst_stats[inst].steps : s.stats->steps, s.freeze_after);
     for (int c = threadIdx.x; c < nb; c += NT) {
         short cs[8];
         lds_slots(sSlot + c * a.Wp, a.Wp, cs);
@@ -433,27 +435,34 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
             e2 = kh * kh * kh;
         }
         const T eps = T(1e-9);
-        T out[8];
+        T out[8], phis[4];
+        if (lmode == LIM_FROZEN) ld_cell(s.phiF, a.ps, base + c, phis);
 #pragma unroll
         for (int v = 0; v < 4; v++) {
             const T gx = G[v][0] * iv, gy = G[v][1] * iv;
             T phi = T(1);
+            if (lmode == LIM_FROZEN) {
+                phi = phis[v];
+            } else {
 #pragma unroll
-            for (int k = 0; k < W; k++) {
-                if (cs[k] < 0) continue;
-                const T d = gx * ro[k][0] + gy * ro[k][1];
-                T pf = T(1);
-                if (s.limiter == LIM_BJ) {                       // Limiter.cpp:67-71
-                    // one division: the numerator is picked by the sign of d
-                    if (d > eps || d < -eps) pf = fmin(T(1), ((d > eps) ? umax[v] - u[v] : umin[v] - u[v]) / d);
-                } else {
-                    if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
+                for (int k = 0; k < W; k++) {
+                    if (cs[k] < 0) continue;
+                    const T d = gx * ro[k][0] + gy * ro[k][1];
+                    T pf = T(1);
+                    if (s.limiter == LIM_BJ) {                       // Limiter.cpp:67-71
+                        // one division: the numerator is picked by the sign of d
+                        if (d > eps || d < -eps) pf = fmin(T(1), ((d > eps) ? umax[v] - u[v] : umin[v] - u[v]) / d);
+                    } else {
+                        if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
+                    }
+                    phi = fmin(phi, pf);
                 }
-                phi = fmin(phi, pf);
             }
+            phis[v] = phi;
             out[2 * v] = phi * gx;
             out[2 * v + 1] = phi * gy;
         }
+        if (lmode == LIM_RECORD) st_cell(s.phiF, a.ps, base + c, phis);
         st_grad(s.phiG, a.ps, base + c, out);
         if (s.time_mode != TM_FIXED) dtc = fmin(dtc, (double) (T(1) / (iv * lam)));
     }

@@ -40,7 +40,7 @@ class WedgeSpec(ct.Structure):
 class Params(ct.Structure):
     _fields_ = [("gma", ct.c_double), ("limiter", ct.c_int), ("venkat_K", ct.c_double),
                 ("precision", ct.c_int), ("block", ct.c_int), ("kernel", ct.c_int), ("tile", ct.c_int),
-                ("keep_numbering", ct.c_int)]
+                ("keep_numbering", ct.c_int), ("freeze_limiter_after", ct.c_longlong)]
 
 
 class StepStats(ct.Structure):
@@ -51,7 +51,7 @@ class StepStats(ct.Structure):
 class ArenaParams(ct.Structure):
     _fields_ = [("hbm_budget", ct.c_size_t), ("precision", ct.c_int), ("limiter", ct.c_int),
                 ("venkat_K", ct.c_double), ("gma", ct.c_double), ("time_mode", ct.c_int), ("tile", ct.c_int),
-                ("slots", ct.c_int), ("max_instances", ct.c_int)]
+                ("slots", ct.c_int), ("max_instances", ct.c_int), ("freeze_limiter_after", ct.c_longlong)]
 
 
 class ArenaInfo(ct.Structure):

@@ -6,9 +6,10 @@ same mesh, both on the GPU, both run to convergence.
                                                  --cfl 0.8 --orders 8 --max-steps 50000]
 
 Defaults are the 1025 x 513-node wedge (1,048,576 triangles), M 3.0, ramp 20 degrees, local
-time stepping at CFL 0.8, Venkatakrishnan limiter K = 5 (with Barth-Jespersen the residual
-stalls after about half an order, the limiter switching back and forth), stop when the L2 density residual has dropped `orders` orders
-below its first value or after `max-steps`.  Prints one JSON object: for each precision the
+time stepping at CFL 0.8, Venkatakrishnan limiter K = 5, stop when the L2 density residual
+has dropped `orders` orders below its first value or after `max-steps`.  Without limiter
+freezing (--freeze N: steps after N reuse step N's limiter values) the residual of either
+limiter stalls after one or two orders, the limiter switching back and forth.  Prints one JSON object: for each precision the
 steps and device time to convergence, and the FP32 errors against FP64 — relative L-inf and
 L2 of each conserved variable, and the L-inf and L2 error of the wall pressure coefficient
 on the lower wall (the ramp).
@@ -28,10 +29,11 @@ LOWER_WALL = 2   # colour of the lower wall (the ramp) in the generated wedge
 
 
 def converge(mesh: Mesh, precision: int, mach: float, cfl: float, orders: float, max_steps: int,
-             mode: int = LOCAL_CFL, limiter: int = LIMITER_VENKAT, K: float = 5.0, chunk: int = 200) -> dict:
+             mode: int = LOCAL_CFL, limiter: int = LIMITER_VENKAT, K: float = 5.0, chunk: int = 200,
+             freeze: int = 0) -> dict:
     """Runs one solve to convergence; returns its state, wall Cp and timing."""
     bcmap, qbc, q = wedge_case(mach)
-    s = Solver(mesh, limiter=limiter, venkat_K=K, precision=precision)
+    s = Solver(mesh, limiter=limiter, venkat_K=K, precision=precision, freeze_limiter_after=freeze)
     s.gather_bcs(bcmap, qbc)
     s.initialise(q)
     steps, ms, hist = 0, 0.0, []
@@ -65,16 +67,17 @@ def errors(a: dict, b: dict) -> dict:
 
 
 def study(nx=1025, ny=513, mach=3.0, theta=20.0, cfl=0.8, orders=8.0, max_steps=50000, seed=1234,
-          mode=LOCAL_CFL, limiter=LIMITER_VENKAT, K=5.0) -> dict:
+          mode=LOCAL_CFL, limiter=LIMITER_VENKAT, K=5.0, freeze=0) -> dict:
     mesh = Mesh.wedge(nx, ny, theta_deg=theta, seed=seed, numbering=NUMBER_RANDOM)
     out = dict(workload=dict(nx=nx, ny=ny, triangles=2 * (nx - 1) * (ny - 1), mach=mach, theta_deg=theta, cfl=cfl,
                              time_mode="local" if mode == LOCAL_CFL else "global", orders=orders,
                              max_steps=max_steps, limiter="venkatakrishnan" if limiter == LIMITER_VENKAT else "bj",
-                             K=K))
+                             K=K, freeze_limiter_after=freeze))
     runs = {}
     for name, prec in (("fp64", FP64), ("fp32", FP32)):
         t0 = time.perf_counter()
-        runs[name] = converge(mesh, prec, mach, cfl, orders, max_steps, mode=mode, limiter=limiter, K=K)
+        runs[name] = converge(mesh, prec, mach, cfl, orders, max_steps, mode=mode, limiter=limiter, K=K,
+                              freeze=freeze)
         r = runs[name]
         out[name] = dict(steps=r["steps"], device_ms=r["ms"], wall_s=time.perf_counter() - t0,
                          residual_drop_orders=r["drop"], converged=bool(r["drop"] is not None and r["drop"] >= orders))
@@ -94,10 +97,12 @@ def main():
     ap.add_argument("--global-dt", action="store_true", help="global instead of local time stepping")
     ap.add_argument("--bj", action="store_true", help="Barth-Jespersen instead of Venkatakrishnan")
     ap.add_argument("--K", type=float, default=5.0)
+    ap.add_argument("--freeze", type=int, default=0,
+                    help="freeze the limiter after this many steps (0: never)")
     a = ap.parse_args()
     print(json.dumps(study(a.nx, a.ny, a.mach, a.theta, a.cfl, a.orders, a.max_steps,
                            mode=GLOBAL_CFL if a.global_dt else LOCAL_CFL,
-                           limiter=LIMITER_BJ if a.bj else LIMITER_VENKAT, K=a.K)))
+                           limiter=LIMITER_BJ if a.bj else LIMITER_VENKAT, K=a.K, freeze=a.freeze)))
 
 
 if __name__ == "__main__":

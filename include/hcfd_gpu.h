@@ -136,6 +136,9 @@ typedef struct hcfd_params {
     int    kernel;      /* enum hcfd_kernel                                                  */
     int    tile;        /* cells per tile of the tiled kernels (32..512, multiple of 32), 0 = 128 */
     int    keep_numbering; /* 1: keep the input cell order on the device instead of the Morton order */
+    long long freeze_limiter_after; /* limiter freezing (not in the reference): steps 1..N compute
+                           the limiter, later steps reuse step N's limiter values with fresh
+                           gradients, counted from hcfd_gpu_initialise; 0 = never        */
 } hcfd_params;
 
 /* Step kernels.  HCFD_KERNEL_TILED (default): persistent CTAs stage tiles of cells, their
@@ -235,6 +238,7 @@ typedef struct hcfd_arena_params {
     int    tile;            /* cells per tile (32..256, multiple of 32), 0 = 128            */
     int    slots;           /* faces per cell: 3 (triangles) or 4 (quads), 0 = 3            */
     int    max_instances;   /* instance slots                                               */
+    long long freeze_limiter_after; /* as in hcfd_params, counted per instance from admission */
 } hcfd_arena_params;
 typedef struct hcfd_arena_info_t {
     size_t cell_capacity, cells_used, face_capacity, faces_used;

@@ -136,7 +136,7 @@ public:
         : Nc(domain.Nc), Nf(domain.Nf), nvars(nvars), domain(domain), flux(flux) {
         (void) grads;
         if (nvars != 4) throw std::runtime_error("hcfd: nvars must be 4 (2-D Euler)");
-        hcfd_params p{flux.gma, limiter.kind, limiter.K, precision, 0, kernel, 0, 0};
+        hcfd_params p{flux.gma, limiter.kind, limiter.K, precision, 0, kernel, 0, 0, 0};
         check(hcfd_gpu_create(&domain.view, &p, &solver_));
         for (int v = 0; v < 4; v++) {
             qbuf_[v].assign(Nc, 0.0);

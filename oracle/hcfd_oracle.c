@@ -36,6 +36,7 @@ struct hcfd_oracle {
     int* bc_type; int* bc_F1; int* bc_F2;
     double (*QBC)[NV]; double (*UBC)[NV];
     int limiter; double K;
+    long long nsteps, freeze_after;
 };
 
 static inline double dot2(const double* a, const double* b) { return a[0]*b[0] + a[1]*b[1]; }
@@ -240,6 +241,15 @@ int hcfd_oracle_initialise(hcfd_oracle* o, const double* qic) {
     for (int v = 0; v < NV; v++)
         for (int i = 0; i < o->Nc; i++) o->U[v][i] = UIC[v];
     update_bc_cells(o);
+    o->nsteps = 0;
+    return 0;
+}
+
+/* Limiter freezing (not in the reference): steps 1..after compute the limiter as usual; every
+ * later step reuses the limiter values of step `after` with fresh gradients.  0 = never. */
+int hcfd_oracle_set_freeze(hcfd_oracle* o, long long after) {
+    if (after < 0) return -1;
+    o->freeze_after = after;
     return 0;
 }
 
@@ -461,7 +471,8 @@ int hcfd_oracle_step(hcfd_oracle* o, int mode, double dt_or_cfl, double* dt_used
             for (int i = 0; i < Nc; i++) o->dtloc[i] *= dt_or_cfl;
     }
     gradient(o);
-    limiter(o);
+    o->nsteps++;
+    if (o->freeze_after <= 0 || o->nsteps <= o->freeze_after) limiter(o);
     bc_grads_limiter(o);
     flux(o);
     if (res_l2) {

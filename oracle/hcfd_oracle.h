@@ -38,6 +38,9 @@ void hcfd_oracle_free(hcfd_oracle* o);
 int hcfd_oracle_gather_bcs(hcfd_oracle* o, const int* bcmap, int nbcmap, const double* qbc);
 /* Euler::initialise (src/Base/Euler.cpp:62-77). */
 int hcfd_oracle_initialise(hcfd_oracle* o, const double* qic);
+/* Limiter freezing: steps 1..after compute the limiter; later steps reuse step `after`'s
+ * limiter values with fresh gradients (0 = never freeze). */
+int hcfd_oracle_set_freeze(hcfd_oracle* o, long long after);
 /* kind HCFD_OR_BJ (src/Base/Limiter.cpp:19-77) or HCFD_OR_VENKAT with constant K. */
 int hcfd_oracle_set_limiter(hcfd_oracle* o, int kind, double K);
 /* One step.  mode HCFD_OR_FIXED_DT uses dt_or_cfl as dt (the reference's only mode);

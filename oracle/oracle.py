@@ -121,6 +121,7 @@ class Oracle:
             L.hcfd_oracle_gather_bcs.argtypes = [ct.c_void_p, _ip, ct.c_int, _dp]
             L.hcfd_oracle_initialise.argtypes = [ct.c_void_p, _dp]
             L.hcfd_oracle_set_limiter.argtypes = [ct.c_void_p, ct.c_int, ct.c_double]
+            L.hcfd_oracle_set_freeze.argtypes = [ct.c_void_p, ct.c_longlong]
             L.hcfd_oracle_step.argtypes = [ct.c_void_p, ct.c_int, ct.c_double, _dp, _dp]
             L.hcfd_oracle_phase.argtypes = [ct.c_void_p, ct.c_int, ct.c_double]
             L.hcfd_oracle_get.argtypes = [ct.c_void_p, ct.c_int, _dp]
@@ -163,6 +164,10 @@ class Oracle:
     def set_limiter(self, kind, K=0.0):
         if self.lib().hcfd_oracle_set_limiter(self.h, kind, K) != 0:
             raise ValueError("oracle: bad limiter")
+
+    def set_freeze(self, after):
+        if self.lib().hcfd_oracle_set_freeze(self.h, after) != 0:
+            raise ValueError("oracle: bad freeze step")
 
     def step(self, mode=FIXED_DT, dt_or_cfl=1e-3):
         dt = np.zeros(1)

@@ -94,3 +94,20 @@ def test_arena_fp32_tracks_the_fp64_oracle():
     for _ in range(50):
         o.step(O.GLOBAL_CFL, 0.5)
     assert np.all(O.rel_linf(a.fetch(k), o.U()) <= 1e-5)
+
+
+def test_arena_limiter_freezing_per_instance():
+    """Instances admitted at different times freeze their limiter after their own N steps."""
+    m1, m2 = H.Mesh.wedge(81, 41, seed=11), H.Mesh.wedge(61, 31, seed=12)
+    bcmap, qbc, q = H.wedge_case(2.5)
+    a = Arena(1 << 27, precision=H.FP64, freeze_limiter_after=15)
+    k1 = a.admit(m1, bcmap, qbc, q, 0.5)
+    a.step(10)
+    k2 = a.admit(m2, bcmap, qbc, q, 0.5)
+    a.step(20)
+    for k, m, n in ((k1, m1, 30), (k2, m2, 20)):
+        s = H.Solver(m, precision=H.FP64, freeze_limiter_after=15)
+        s.gather_bcs(bcmap, qbc)
+        s.initialise(q)
+        s.step(n, H.GLOBAL_CFL, 0.5)
+        assert np.array_equal(a.fetch(k), s.U())

@@ -202,3 +202,29 @@ def test_kernel_families_and_orders_agree(precision, tile):
     tol = 1e-13 if precision == H.FP64 else 1e-6
     for r in runs[1:]:
         assert np.all(O.rel_linf(r, runs[0]) <= tol)
+
+
+@pytest.mark.parametrize("kernel", [H.KERNEL_TILED, H.KERNEL_CELL])
+@pytest.mark.parametrize("limiter,K", [(H.LIMITER_BJ, 0.0), (H.LIMITER_VENKAT, 5.0)])
+def test_limiter_freezing_matches_oracle(kernel, limiter, K):
+    """Limiter freezing (not in the reference): steps 1..N compute the limiter, later steps
+    reuse step N's values; the GPU's device-side step count must switch at the same step.
+    The oracle restarts each step from the GPU's state, so the comparison is per step and
+    rounding differences cannot build up through the limiter's switches."""
+    m = H.Mesh.wedge(81, 41, theta_deg=20.0, seed=1234, numbering=H.NUMBER_RANDOM)
+    case = H.wedge_case(3.0)
+    s = solver_for(m, *case, limiter=limiter, venkat_K=K, kernel=kernel, freeze_limiter_after=25)
+    free = solver_for(m, *case, limiter=limiter, venkat_K=K, kernel=kernel)
+    o = oracle_for(m, *case, limiter=limiter, K=K)
+    o.set_freeze(25)
+    for i in range(1, 41):
+        o.set_U(s.U())
+        st = s.step(1, H.LOCAL_CFL, 0.8)
+        dt_o, res_o = o.step(O.LOCAL_CFL, 0.8)
+        free.step(1, H.LOCAL_CFL, 0.8)
+        assert abs(st["res_l2"] - res_o) <= 1e-11 * res_o, i
+        assert np.all(O.rel_linf(s.U(), o.U()) <= 1e-11), i
+        if i <= 25:
+            assert np.array_equal(s.U(), free.U()), i     # the same kernels before the switch
+        elif i == 26:
+            assert not np.array_equal(s.U(), free.U())   # the frozen limiter is in use
