@@ -48,6 +48,31 @@ class Arena:
         self._nc[slot.value] = v.Nc
         return slot.value
 
+    def prepare(self, mesh: Mesh, bcmap, qbc, qic, dt_or_cfl: float) -> "Admission":
+        """The host half of admit (tile plan, BC table); safe to call from worker threads
+        while another thread steps the arena."""
+        v = mesh.view()
+        bm = np.ascontiguousarray(bcmap, dtype=np.int32)
+        q = np.ascontiguousarray(qbc, dtype=np.float64).reshape(-1)
+        qi = np.ascontiguousarray(qic, dtype=np.float64)
+        h = ct.c_void_p()
+        _n.check(_n.lib().hcfd_arena_prepare(self._h, ct.byref(v), bm.ctypes.data_as(_n._ip), len(bm),
+                                             q.ctypes.data_as(_n._dp), qi.ctypes.data_as(_n._dp), dt_or_cfl,
+                                             ct.byref(h)))
+        return Admission(h, mesh, v.Nc)
+
+    def admit_prepared(self, adm: "Admission"):
+        """The device half of admit; returns the slot, or None when the arena is full (the
+        admission stays usable)."""
+        slot = ct.c_int()
+        rc = _n.lib().hcfd_arena_admit_prepared(self._h, adm._h, ct.byref(slot))
+        if rc == _n.EAGAIN:
+            return None
+        _n.check(rc)
+        self._mesh[slot.value] = adm.mesh
+        self._nc[slot.value] = adm.Nc
+        return slot.value
+
     def step(self, nsteps: int) -> None:
         _n.check(_n.lib().hcfd_arena_step(self._h, nsteps))
 
@@ -75,3 +100,19 @@ class Arena:
         i = _n.ArenaInfo()
         _n.check(_n.lib().hcfd_arena_info(self._h, ct.byref(i)))
         return {k: getattr(i, k) for k, _ in _n.ArenaInfo._fields_}
+
+
+class Admission:
+    """A prepared admission (hcfd_arena_prepare); holds the mesh it was built from."""
+
+    def __init__(self, h, mesh: Mesh, Nc: int):
+        self._h = h
+        self.mesh = mesh
+        self.Nc = Nc
+        self.cells = int(_n.lib().hcfd_admission_cells(h))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _n.lib().hcfd_admission_free(h)
+            self._h = None

@@ -1,12 +1,16 @@
 """Autotuner of the step kernels' launch shape, cached per GPU, precision, limiter and size
 class.
 
-Candidates: the tiled kernels with 64, 128 or 256 cells per tile (one compute thread per
-cell, or 128 threads over 256 cells — two cells per thread), and the per-cell kernels with
-128 or 256 threads per block (no tile staging: the other fusion split).  A size class is
-round(log2(real cells)); each class is tuned once on a supersonic wedge of about that many
-triangles and the winner is stored in a JSON cache ($HCFD_AUTOTUNE_CACHE, default
-~/.cache/hcfd_b200/autotune.json).
+Two tunings:
+  - a single-mesh solver (Solver): the tiled kernels with 64, 128 or 256 cells per tile
+    (one compute thread per cell, or 128 threads over 256 cells — two cells per thread)
+    against the per-cell kernels with 128 or 256 threads per block (no tile staging: the
+    other fusion split), timed on one wedge of the size class;
+  - an arena (Arena): its tile size (64, 128 or 256 cells, one thread per cell), timed on
+    an arena holding copies of a wedge of the size class, about 2 million cells in all, so
+    that the timing is that of a full device and not of one launch-bound instance.
+A size class is round(log2(real cells)), clamped to [10, 24].  The winners are stored in a
+JSON cache ($HCFD_AUTOTUNE_CACHE, default ~/.cache/hcfd_b200/autotune.json).
 """
 from __future__ import annotations
 
@@ -14,11 +18,12 @@ import json
 import math
 import os
 import subprocess
+import time
 
-from . import (FP32, FP64, GLOBAL_CFL, KERNEL_CELL, KERNEL_TILED, LIMITER_BJ, NUMBER_RANDOM, Mesh, Solver,
+from . import (FP64, GLOBAL_CFL, KERNEL_CELL, KERNEL_TILED, LIMITER_BJ, NUMBER_RANDOM, Mesh, Solver, device_sync,
                wedge_case)
 
-CANDIDATES = (
+SOLVER_SHAPES = (
     dict(kernel=KERNEL_TILED, tile=64, block=64),
     dict(kernel=KERNEL_TILED, tile=128, block=128),
     dict(kernel=KERNEL_TILED, tile=256, block=256),
@@ -26,6 +31,7 @@ CANDIDATES = (
     dict(kernel=KERNEL_CELL, tile=0, block=128),
     dict(kernel=KERNEL_CELL, tile=0, block=256),
 )
+ARENA_TILES = (64, 128, 256)
 
 
 def cache_path() -> str:
@@ -37,7 +43,7 @@ def gpu_name() -> str:
     try:
         out = subprocess.run(["nvidia-smi", "--query-gpu=name", "--format=csv,noheader", "-i", "0"],
                              capture_output=True, text=True, timeout=20).stdout.strip()
-        return out or "unknown"
+        return out.splitlines()[0] if out else "unknown"
     except (OSError, subprocess.SubprocessError):
         return "unknown"
 
@@ -46,8 +52,14 @@ def size_class(ncells: int) -> int:
     return max(10, min(24, int(round(math.log2(max(ncells, 2))))))
 
 
-def _key(cls: int, precision: int, limiter: int, arena_shapes: bool) -> str:
-    return f"{gpu_name()}|{'fp32' if precision == FP32 else 'fp64'}|lim{limiter}|c{cls}|{'arena' if arena_shapes else 'all'}"
+def class_mesh(cls: int) -> Mesh:
+    """A wedge on a 2:1 node grid with about 2**cls triangles."""
+    ny1 = max(2, int(round(math.sqrt(2 ** cls / 4.0))))
+    return Mesh.wedge(2 * ny1 + 1, ny1 + 1, seed=4321, numbering=NUMBER_RANDOM)
+
+
+def _key(kind: str, cls: int, precision: int, limiter: int) -> str:
+    return f"{gpu_name()}|{kind}|{'fp64' if precision == FP64 else 'fp32'}|lim{limiter}|c{cls}"
 
 
 def _load() -> dict:
@@ -67,39 +79,71 @@ def _store(d: dict) -> None:
     os.replace(tmp, p)
 
 
-def tune_class(cls: int, precision: int = FP64, limiter: int = LIMITER_BJ, steps: int = 40,
-               arena_shapes: bool = False) -> dict:
-    """Times every candidate on a wedge of about 2**cls triangles; returns the timings.
-    With `arena_shapes` only the shapes an arena can run (tiled, one thread per cell)."""
-    ny1 = max(2, int(round(math.sqrt(2 ** cls / 4.0))))
-    mesh = Mesh.wedge(2 * ny1 + 1, ny1 + 1, seed=4321, numbering=NUMBER_RANDOM)
+def tune_solver(cls: int, precision: int = FP64, limiter: int = LIMITER_BJ, steps: int = 40) -> dict:
+    """Times every solver shape on one wedge of the class; returns the timings, best first."""
+    mesh = class_mesh(cls)
     bcmap, qbc, q = wedge_case(2.5)
     res = []
-    for c in CANDIDATES:
-        if arena_shapes and (c["kernel"] != KERNEL_TILED or c["block"] != c["tile"]):
-            continue
+    for c in SOLVER_SHAPES:
         s = Solver(mesh, precision=precision, limiter=limiter, **c)
         s.gather_bcs(bcmap, qbc)
         s.initialise(q)
         s.step(5, GLOBAL_CFL, 0.5)
-        ms = s.step_timed(steps, GLOBAL_CFL, 0.5) / steps
-        res.append(dict(c, ms_per_step=ms))
+        res.append(dict(c, ms_per_step=s.step_timed(steps, GLOBAL_CFL, 0.5) / steps))
         del s
     res.sort(key=lambda r: r["ms_per_step"])
     return dict(best=res[0], timings=res, cells=mesh.Nc)
 
 
-def best(ncells: int, precision: int = FP64, limiter: int = LIMITER_BJ, tune: bool = True,
-         arena_shapes: bool = False) -> dict:
-    """The cached winner for this size class ({kernel, tile, block}); tunes and caches it
-    when missing and `tune` is true, else returns the default shape."""
+def tune_arena(cls: int, precision: int, limiter: int = LIMITER_BJ, steps: int = 40,
+               target_cells: int = 2_000_000) -> dict:
+    """Times every arena tile size on an arena of copies of a wedge of the class."""
+    from .arena import Arena
+    mesh = class_mesh(cls)
+    copies = max(1, min(512, target_cells // mesh.Nc))
+    bcmap, qbc, q = wedge_case(2.5)
+    res = []
+    for tile in ARENA_TILES:
+        a = Arena(int(max(1e9, 600.0 * copies * mesh.Nc)), precision=precision, limiter=limiter, tile=tile,
+                  max_instances=copies)
+        for _ in range(copies):
+            if a.admit(mesh, bcmap, qbc, q, 0.5) is None:
+                raise RuntimeError("autotune: arena full")
+        a.step(4)
+        a.poll()
+        device_sync()
+        t0 = time.perf_counter()
+        a.step(steps)
+        a.poll()
+        res.append(dict(tile=tile, ms_per_step=1e3 * (time.perf_counter() - t0) / steps))
+        del a
+    res.sort(key=lambda r: r["ms_per_step"])
+    return dict(best=res[0], timings=res, cells=mesh.Nc, copies=copies)
+
+
+def best_solver_shape(ncells: int, precision: int = FP64, limiter: int = LIMITER_BJ, tune: bool = True) -> dict:
+    """The cached winner for a single mesh of this size ({kernel, tile, block}); tuned and
+    cached when missing and `tune` is true, else the default shape."""
     cls = size_class(ncells)
-    key = _key(cls, precision, limiter, arena_shapes)
+    key = _key("solver", cls, precision, limiter)
     d = _load()
     if key not in d:
         if not tune:
             return dict(kernel=KERNEL_TILED, tile=128, block=128)
-        d[key] = tune_class(cls, precision, limiter, arena_shapes=arena_shapes)
+        d[key] = tune_solver(cls, precision, limiter)
         _store(d)
     b = d[key]["best"]
     return dict(kernel=b["kernel"], tile=b["tile"], block=b["block"])
+
+
+def best_arena_tile(ncells: int, precision: int, limiter: int = LIMITER_BJ, tune: bool = True) -> int:
+    """The cached arena tile size for instances of about this size."""
+    cls = size_class(ncells)
+    key = _key("arena", cls, precision, limiter)
+    d = _load()
+    if key not in d:
+        if not tune:
+            return 128
+        d[key] = tune_arena(cls, precision, limiter)
+        _store(d)
+    return int(d[key]["best"]["tile"])

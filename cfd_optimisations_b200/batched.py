@@ -92,13 +92,13 @@ def main():
     t_gen = time.perf_counter() - t0
     real = [m.Nc - (2 * (s["nx"] - 1) + 2 * (s["ny"] - 1)) for m, s in zip(meshes, specs)]
     median = int(np.median(real))
-    shape = autotune.best(median, FP32, LIMITER_BJ, arena_shapes=True)
-    arena, slots, stats, t_admit, t_run = run_arena(meshes, specs, a.steps, tile=shape["tile"])
+    tile = autotune.best_arena_tile(median, FP32, LIMITER_BJ)
+    arena, slots, stats, t_admit, t_run = run_arena(meshes, specs, a.steps, tile=tile)
     upd = sum(real) * (a.steps - 2)
     out = dict(workload=dict(instances=a.instances, steps=a.steps, triangles_total=int(sum(real)),
                              triangles_median=median, seed=a.seed, limiter="barth-jespersen", cfl=0.5),
                mesh_generation_s=t_gen,
-               arena=dict(precision="fp32-compensated", tile=shape["tile"], admit_s=t_admit, run_s=t_run,
+               arena=dict(precision="fp32-compensated", tile=tile, admit_s=t_admit, run_s=t_run,
                           cell_updates_per_s=upd / t_run, solves_per_s=a.instances / t_run,
                           nonfinite=sum(1 for s in stats.values() if s["nonfinite"])))
     if not a.no_loop:

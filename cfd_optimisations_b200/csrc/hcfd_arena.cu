@@ -137,6 +137,19 @@ __global__ void arena_iv_kernel(int n, const double* __restrict__ ivu, const int
     if (i < n) iv[i] = T(ivu[perm[i]]);
 }
 
+// dst[k] = c0 + map[src[k]]: input cell numbers -> arena cell numbers.
+__global__ void arena_cellmap_kernel(long long n, int c0, const int* __restrict__ map, const int* __restrict__ src,
+                                     int* __restrict__ dst) {
+    const long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[k] = c0 + map[src[k]];
+}
+
+// dst[k] = c0 + src[k]: tile-local halo cell numbers -> arena cell numbers.
+__global__ void arena_offset_kernel(long long n, int c0, const int* __restrict__ src, int* __restrict__ dst) {
+    const long long k = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[k] = c0 + src[k];
+}
+
 }  // namespace
 
 
@@ -178,6 +191,19 @@ struct hcfd_arena {
     int graph_steps = 0;
     long long steps_done = 0;
     bool fp32() const { return prm.precision == HCFD_FP32; }
+};
+
+// The host half of an admission (hcfd_arena_prepare): everything that does not depend on
+// where in the arena the mesh lands.  The mesh arrays are the caller's.
+struct hcfd_admission {
+    const hcfd_arena* owner = nullptr;
+    hcfd_mesh_view mv{};
+    int Nc = 0, Nf = 0, F_BC = 0, nreal = 0;
+    std::vector<int> cf_off, cf_con, perm, iperm;
+    hcfd::TilePlan P;
+    hcfd::BCTable bc{};
+    double u0[4] = {0, 0, 0, 0};
+    double dt = 0;
 };
 
 namespace {
@@ -331,7 +357,7 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
     CK(cudaDeviceGetAttribute(&A->nsm, cudaDevAttrMultiProcessorCount, A->device));
     A->B = p.tile ? p.tile : 128;
     A->W = p.slots == 4 ? 4 : 3;
-    A->Wp = 4;
+    A->Wp = A->W;
     A->time_mode = p.time_mode;
     // per-tile staging capacities (generous for triangle and quad meshes at this tile size)
     A->Hcap = A->B * 7 / 8 + 16;
@@ -340,7 +366,7 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
     const size_t ts = A->tsz;
     // Budget split, bytes per cell: state x2, gradients, iv, slots; ~1.75 face entries per
     // cell (records + metadata) and ~0.6 halo ids per cell, as the wedge meshes need.
-    const double per_cell = 2 * 4 * ts + 8 * ts + ts + A->Wp * 2 + 1.75 * (8 * ts + 16) + 0.6 * 4 +
+    const double per_cell = 2 * 4 * ts + 8 * ts + ts + A->Wp * 2 + 1.75 * (8 * ts + 8) + 0.6 * 4 +
                             (p.freeze_limiter_after > 0 ? 4 * ts : 0);
     size_t budget = p.hbm_budget;
     size_t C = (size_t) (budget / per_cell);
@@ -363,7 +389,7 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
         (rc = dalloc((char**) &h->phiG, 8 * ts * C)) || (rc = dalloc((char**) &h->iv, ts * C)) ||
         (p.freeze_limiter_after > 0 && (rc = dalloc((char**) &h->phiF, 4 * ts * C))) ||
         (rc = dalloc(&h->cslot, h->Wp * C)) || (rc = dalloc((char**) &h->tgeo, 8 * ts * h->Ecap)) ||
-        (rc = dalloc(&h->tmeta, 8 * h->Ecap)) || (rc = dalloc(&h->halo, h->HLcap)) ||
+        (rc = dalloc(&h->tmeta, 4 * h->Ecap)) || (rc = dalloc(&h->halo, h->HLcap)) ||
         (rc = dalloc(&h->inst_dt, p.max_instances)) || (rc = dalloc(&h->inst_dtmin, 2 * (size_t) p.max_instances)) ||
         (rc = dalloc(&h->inst_bc, p.max_instances)) || (rc = dalloc(&h->stats, p.max_instances)) ||
         (rc = dalloc(&h->tiles, 2 * h->tiles_cap)) || (rc = dalloc(&h->act, p.max_instances)) ||
@@ -383,49 +409,76 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
     return HCFD_OK;
 }
 
-int hcfd_arena_admit(hcfd_arena* A, const hcfd_mesh_view* mv, const int* bcmap, int nbcmap, const double* qbc,
-                     const double* qic, double dt_or_cfl, int* slot_out) {
+int hcfd_arena_prepare(const hcfd_arena* A, const hcfd_mesh_view* mv, const int* bcmap, int nbcmap, const double* qbc,
+                       const double* qic, double dt_or_cfl, hcfd_admission** out) {
     hcfd::clear_error();
-    if (!A || !mv || !bcmap || !qbc || !qic || !slot_out || !(dt_or_cfl > 0)) return fail(HCFD_EINVAL, "arena_admit: bad argument");
-    CK(cudaSetDevice(A->device));
+    if (!A || !mv || !bcmap || !qbc || !qic || !out || !(dt_or_cfl > 0)) return fail(HCFD_EINVAL, "arena_prepare: bad argument");
+    *out = nullptr;
     int rc = hcfd::validate_view(*mv);
     if (rc) return rc;
-    int slot = -1;
-    for (size_t k = 0; k < A->inst.size(); k++) if (!A->inst[k].active) { slot = (int) k; break; }
-    if (slot < 0) return fail(HCFD_EAGAIN, "arena_admit: all instance slots in use");
+    auto D = std::make_unique<hcfd_admission>();
+    D->owner = A;
+    D->mv = *mv;
     const int Nc = mv->Nc, Nf = mv->Nf, Ncol = mv->Ncol, NBC = mv->NBCcol;
-    if (NBC > hcfd::MAXBC) return fail(HCFD_EINVAL, "arena_admit: more than 16 boundary colours");
+    if (NBC > hcfd::MAXBC) return fail(HCFD_EINVAL, "arena_prepare: more than 16 boundary colours");
     const int F_BC = mv->coloff[Ncol - NBC];
-    std::vector<int> cf_off, cf_con;
-    hcfd::build_cf(Nc, Nf, mv->fc_con, cf_off, cf_con);
+    hcfd::build_cf(Nc, Nf, mv->fc_con, D->cf_off, D->cf_con);
     std::vector<char> ghost(Nc, 0);
     for (int f = F_BC; f < Nf; f++) ghost[mv->fc_con[2 * f + 1]] = 1;
     int nreal = 0, maxdeg = 0;
-    for (int c = 0; c < Nc; c++) if (!ghost[c]) { nreal++; maxdeg = std::max(maxdeg, cf_off[c + 1] - cf_off[c]); }
-    if (maxdeg > A->W) return fail(HCFD_EINVAL, "arena_admit: cells with more faces than the arena's slots");
-    std::vector<int> perm = hcfd::morton_order(*mv);
+    for (int c = 0; c < Nc; c++) if (!ghost[c]) { nreal++; maxdeg = std::max(maxdeg, D->cf_off[c + 1] - D->cf_off[c]); }
+    if (maxdeg > A->W) return fail(HCFD_EINVAL, "arena_prepare: cells with more faces than the arena's slots");
+    D->perm = hcfd::morton_order(*mv);
+    D->iperm.resize(Nc);
+    for (int i = 0; i < Nc; i++) D->iperm[D->perm[i]] = i;
     std::vector<int> bc_first;
     for (int col = Ncol - NBC; col < Ncol; col++) bc_first.push_back(mv->coloff[col]);
-    hcfd::TilePlan P;
-    rc = hcfd::build_tile_plan(*mv, cf_off, cf_con, ghost, perm, F_BC, bc_first, A->B, A->W, P);
+    rc = hcfd::build_tile_plan(*mv, D->cf_off, D->cf_con, ghost, D->perm, F_BC, bc_first, A->B, A->W, D->P);
     if (rc) return rc;
-    if (P.Hmax > A->Hcap || P.Fmax > A->Fcap) return fail(HCFD_EINVAL, "arena_admit: a tile's halo or faces exceed the arena's staging capacity");
+    if (D->P.Hmax > A->Hcap || D->P.Fmax > A->Fcap)
+        return fail(HCFD_EINVAL, "arena_prepare: a tile's halo or faces exceed the arena's staging capacity");
     // BC table (Euler::gather_BCs, src/Base/Euler.cpp:42-60)
-    hcfd::BCTable bc{};
+    hcfd::BCTable& bc = D->bc;
+    bc = hcfd::BCTable{};
     bc.nbc = NBC;
     for (int col = Ncol - NBC; col < Ncol; col++) {
         const int b = col - (Ncol - NBC), tag = mv->coltag[col];
         if (tag < 0 || tag >= nbcmap || bcmap[tag] < HCFD_SYMMETRY || bcmap[tag] > HCFD_SUBOUTLET)
-            return fail(HCFD_EINVAL, "arena_admit: bad BC map");
+            return fail(HCFD_EINVAL, "arena_prepare: bad BC map");
         bc.type[b] = bcmap[tag];
         bc.F1[b] = mv->coloff[col];
         for (int v = 0; v < 4; v++) bc.QBC[b][v] = qbc[4 * b + v];
         prim_to_cons(bc.QBC[b], A->prm.gma, bc.UBC[b]);
     }
     bc.F1[NBC] = Nf;
+    // initial state (Euler::initialise, src/Base/Euler.cpp:62-77)
+    prim_to_cons(qic, A->prm.gma, D->u0);
+    D->Nc = Nc; D->Nf = Nf; D->F_BC = F_BC; D->nreal = nreal;
+    D->dt = dt_or_cfl;
+    *out = D.release();
+    return HCFD_OK;
+}
+
+size_t hcfd_admission_cells(const hcfd_admission* D) {
+    return D && D->owner ? (size_t) D->P.ntiles * D->owner->B : 0;
+}
+
+void hcfd_admission_free(hcfd_admission* D) { delete D; }
+
+int hcfd_arena_admit_prepared(hcfd_arena* A, const hcfd_admission* D, int* slot_out) {
+    hcfd::clear_error();
+    if (!A || !D || !slot_out) return fail(HCFD_EINVAL, "arena_admit: bad argument");
+    if (D->owner != A) return fail(HCFD_EINVAL, "arena_admit: the admission was prepared for another arena");
+    CK(cudaSetDevice(A->device));
+    int slot = -1;
+    for (size_t k = 0; k < A->inst.size(); k++) if (!A->inst[k].active) { slot = (int) k; break; }
+    if (slot < 0) return fail(HCFD_EAGAIN, "arena_admit: all instance slots in use");
+    const hcfd_mesh_view* mv = &D->mv;
+    const hcfd::TilePlan& P = D->P;
+    const int Nc = D->Nc, Nf = D->Nf, F_BC = D->F_BC;
     // ranges in the arena (budget admission)
     Inst I;
-    I.Nc = Nc; I.Nf = Nf; I.Nreal = nreal; I.ntiles = P.ntiles;
+    I.Nc = Nc; I.Nf = Nf; I.Nreal = D->nreal; I.ntiles = P.ntiles;
     I.ncell = (size_t) P.ntiles * A->B;
     I.ne = P.efid.size();
     I.nh = P.halo.size();
@@ -450,56 +503,55 @@ int hcfd_arena_admit(hcfd_arena* A, const hcfd_mesh_view* mv, const int* bcmap, 
         d[5] = P.hoff[t + 1] - P.hoff[t];
         d[6] = d[7] = 0;
     }
-    std::vector<int> halo_g(P.halo.size());
-    for (size_t k = 0; k < P.halo.size(); k++) halo_g[k] = (int) (I.c0 + P.halo[k]);
-    std::vector<int> iperm(Nc);
-    for (int i = 0; i < Nc; i++) iperm[perm[i]] = i;
-    std::vector<int> fc_g(2 * (size_t) Nf);
-    for (size_t k = 0; k < fc_g.size(); k++) fc_g[k] = (int) (I.c0 + iperm[mv->fc_con[k]]);
-    std::vector<int> foff_rel(P.foff);
-    // device work: geometry of this mesh (temporaries), then the arena ranges
+    // device work: geometry of this mesh (stream-ordered temporaries), then the arena ranges
     cudaStream_t st = A->stream;
     int *d_fn = nullptr, *d_fcu = nullptr, *d_fcg = nullptr, *d_cnoff = nullptr, *d_cncon = nullptr, *d_cfoff = nullptr,
-        *d_cfcon = nullptr, *d_efid = nullptr, *d_foff = nullptr;
+        *d_cfcon = nullptr, *d_efid = nullptr, *d_foff = nullptr, *d_iperm = nullptr, *d_halo = nullptr;
     double *d_nodes = nullptr, *d_xc = nullptr, *d_ivu = nullptr;
     hcfd::FaceGeo<double>* d_geo = nullptr;
     const int ncn = mv->cn_off[Nc];
-    auto tmp_free = [&]() {
-        cudaStreamSynchronize(st);
-        void* t[] = {d_fn, d_fcu, d_fcg, d_cnoff, d_cncon, d_cfoff, d_cfcon, d_efid, d_foff, d_nodes, d_xc, d_ivu, d_geo};
-        for (void* q : t) if (q) cudaFree(q);
+    cudaError_t ce = cudaSuccess;
+    auto tmp = [&](auto** p, size_t n) {
+        if (ce == cudaSuccess) ce = cudaMallocAsync((void**) p, std::max<size_t>(n, 1) * sizeof(**p), st);
     };
-    if ((rc = dalloc(&d_fn, 2 * (size_t) Nf)) || (rc = dalloc(&d_fcu, 2 * (size_t) Nf)) || (rc = dalloc(&d_fcg, 2 * (size_t) Nf)) ||
-        (rc = dalloc(&d_cnoff, Nc + 1)) || (rc = dalloc(&d_cncon, ncn)) || (rc = dalloc(&d_cfoff, Nc + 1)) ||
-        (rc = dalloc(&d_cfcon, cf_con.size())) || (rc = dalloc(&d_efid, I.ne)) || (rc = dalloc(&d_foff, foff_rel.size())) ||
-        (rc = dalloc(&d_nodes, 2 * (size_t) mv->Nn)) || (rc = dalloc(&d_xc, 2 * (size_t) Nc)) || (rc = dalloc(&d_ivu, Nc)) ||
-        (rc = dalloc(&d_geo, Nf)) || (rc = dalloc(&I.d_perm, Nc))) {
+    tmp(&d_fn, 2 * (size_t) Nf); tmp(&d_fcu, 2 * (size_t) Nf); tmp(&d_fcg, 2 * (size_t) Nf);
+    tmp(&d_cnoff, Nc + 1); tmp(&d_cncon, ncn); tmp(&d_cfoff, Nc + 1); tmp(&d_cfcon, D->cf_con.size());
+    tmp(&d_efid, I.ne); tmp(&d_foff, P.foff.size()); tmp(&d_iperm, Nc); tmp(&d_halo, I.nh);
+    tmp(&d_nodes, 2 * (size_t) mv->Nn); tmp(&d_xc, 2 * (size_t) Nc); tmp(&d_ivu, Nc); tmp(&d_geo, Nf);
+    auto tmp_free = [&]() {
+        void* t[] = {d_fn, d_fcu, d_fcg, d_cnoff, d_cncon, d_cfoff, d_cfcon, d_efid, d_foff, d_iperm, d_halo,
+                     d_nodes, d_xc, d_ivu, d_geo};
+        for (void* q : t) if (q) cudaFreeAsync(q, st);
+    };
+    if (ce == cudaSuccess) ce = cudaMalloc((void**) &I.d_perm, sizeof(int) * (size_t) Nc);
+    if (ce != cudaSuccess) {
         tmp_free();
         if (I.d_perm) cudaFree(I.d_perm);
+        cudaStreamSynchronize(st);
         undo();
-        return rc;
+        return fail(ce == cudaErrorMemoryAllocation ? HCFD_ENOMEM : HCFD_ECUDA,
+                    std::string("arena_admit: ") + cudaGetErrorString(ce));
     }
-    cudaError_t ce = cudaSuccess;
     auto up = [&](void* dst, const void* src, size_t bytes) {
         if (ce == cudaSuccess && bytes) ce = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
     };
     up(d_fn, mv->fn_con, 8 * (size_t) Nf);
     up(d_fcu, mv->fc_con, 8 * (size_t) Nf);
-    up(d_fcg, fc_g.data(), 4 * fc_g.size());
     up(d_cnoff, mv->cn_off, 4 * (size_t) (Nc + 1));
     up(d_cncon, mv->cn_con, 4 * (size_t) ncn);
-    up(d_cfoff, cf_off.data(), 4 * cf_off.size());
-    up(d_cfcon, cf_con.data(), 4 * cf_con.size());
+    up(d_cfoff, D->cf_off.data(), 4 * D->cf_off.size());
+    up(d_cfcon, D->cf_con.data(), 4 * D->cf_con.size());
     up(d_efid, P.efid.data(), 4 * I.ne);
-    up(d_foff, foff_rel.data(), 4 * foff_rel.size());
+    up(d_foff, P.foff.data(), 4 * P.foff.size());
+    up(d_iperm, D->iperm.data(), 4 * (size_t) Nc);
+    up(d_halo, P.halo.data(), 4 * I.nh);
     up(d_nodes, mv->nodes, 16 * (size_t) mv->Nn);
-    up(I.d_perm, perm.data(), 4 * (size_t) Nc);
-    up(A->tmeta + 8 * I.e0, P.meta.data(), 2 * P.meta.size());
+    up(I.d_perm, D->perm.data(), 4 * (size_t) Nc);
+    up(A->tmeta + 4 * I.e0, P.meta.data(), 2 * P.meta.size());
     up(A->cslot + A->Wp * I.c0, P.cslot.data(), 2 * P.cslot.size());
-    up(A->halo + I.h0, halo_g.data(), 4 * halo_g.size());
-    const double inf2[2] = {0, 0};
-    (void) inf2;
     if (ce == cudaSuccess) {
+        arena_cellmap_kernel<<<nblk(2 * (long long) Nf, 256), 256, 0, st>>>(2 * (long long) Nf, (int) I.c0, d_iperm, d_fcu, d_fcg);
+        if (I.nh) arena_offset_kernel<<<nblk((long long) I.nh, 256), 256, 0, st>>>((long long) I.nh, (int) I.c0, d_halo, A->halo + I.h0);
         hcfd::geom_xc_kernel<<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_cnoff, d_cncon, d_nodes, d_xc);
         hcfd::geom_face_kernel<<<nblk(Nf, 256), 256, 0, st>>>(Nf, F_BC, d_fn, d_fcu, d_nodes, d_xc, d_geo);
         hcfd::geom_iv_kernel<<<nblk(Nc, 256), 256, 0, st>>>(Nc, F_BC, d_cfoff, d_cfcon, d_fcu, d_geo, d_ivu);
@@ -511,42 +563,54 @@ int hcfd_arena_admit(hcfd_arena* A, const hcfd_mesh_view* mv, const int* bcmap, 
             arena_iv_kernel<double><<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_ivu, I.d_perm, (double*) A->iv + I.c0);
             hcfd::gather_geo_kernel<double><<<P.ntiles, 128, 0, st>>>(P.ntiles, d_foff, d_efid, d_geo, (double*) A->tgeo + 8 * I.e0);
         }
-        // initial state (Euler::initialise, src/Base/Euler.cpp:62-77) into the current buffer
-        double u[4];
-        prim_to_cons(qic, A->prm.gma, u);
+        // initial state into the current buffer, then the ghost cells from the BCs
+        const double* u = D->u0;
         const int nfill = (int) I.ncell;
         if (A->fp32()) {
             arena_fill_kernel<float><<<nblk(nfill, 256), 256, 0, st>>>(A->Ccap, I.c0, nfill, (Cell4<float>*) A->U[A->cur], u[0], u[1], u[2], u[3]);
             if (Nf > F_BC)
                 hcfd::bc_cells_kernel<float><<<nblk(Nf - F_BC, 256), 256, 0, st>>>((int) A->Ccap, Nf, F_BC, d_fcg, d_geo,
-                                                                                   (Cell4<float>*) A->U[A->cur], float(A->prm.gma), bc);
+                                                                                   (Cell4<float>*) A->U[A->cur], float(A->prm.gma), D->bc);
         } else {
             arena_fill_kernel<double><<<nblk(nfill, 256), 256, 0, st>>>(A->Ccap, I.c0, nfill, (Cell4<double>*) A->U[A->cur], u[0], u[1], u[2], u[3]);
             if (Nf > F_BC)
                 hcfd::bc_cells_kernel<double><<<nblk(Nf - F_BC, 256), 256, 0, st>>>((int) A->Ccap, Nf, F_BC, d_fcg, d_geo,
-                                                                                    (Cell4<double>*) A->U[A->cur], A->prm.gma, bc);
+                                                                                    (Cell4<double>*) A->U[A->cur], A->prm.gma, D->bc);
         }
         if (ce == cudaSuccess) ce = cudaGetLastError();
     }
     const unsigned long long infb[2] = {0x7FF0000000000000ULL, 0x7FF0000000000000ULL};
     up(A->inst_dtmin + 2 * slot, infb, sizeof(infb));
-    up(A->inst_dt + slot, &dt_or_cfl, sizeof(double));
-    up(A->inst_bc + slot, &bc, sizeof(bc));
+    up(A->inst_dt + slot, &D->dt, sizeof(double));
+    up(A->inst_bc + slot, &D->bc, sizeof(hcfd::BCTable));
     if (ce == cudaSuccess) ce = cudaMemsetAsync(A->stats + slot, 0, sizeof(hcfd::StepStats), st);
     tmp_free();
+    // the uploads above read pageable host memory (the stack included): wait for them
+    const cudaError_t se = cudaStreamSynchronize(st);
+    if (ce == cudaSuccess) ce = se;
     if (ce != cudaSuccess) {
         cudaFree(I.d_perm);
         undo();
         return fail(HCFD_ECUDA, std::string("arena_admit: ") + cudaGetErrorString(ce));
     }
-    I.dt = dt_or_cfl;
+    I.dt = D->dt;
     I.active = true;
     I.admitted_step = A->steps_done;
     A->inst[slot] = std::move(I);
-    rc = rebuild_active(A);
+    int rc = rebuild_active(A);
     if (rc) return rc;
     *slot_out = slot;
     return HCFD_OK;
+}
+
+int hcfd_arena_admit(hcfd_arena* A, const hcfd_mesh_view* mv, const int* bcmap, int nbcmap, const double* qbc,
+                     const double* qic, double dt_or_cfl, int* slot_out) {
+    hcfd_admission* D = nullptr;
+    int rc = hcfd_arena_prepare(A, mv, bcmap, nbcmap, qbc, qic, dt_or_cfl, &D);
+    if (rc) return rc;
+    rc = hcfd_arena_admit_prepared(A, D, slot_out);
+    hcfd_admission_free(D);
+    return rc;
 }
 
 int hcfd_arena_step(hcfd_arena* A, int nsteps) {

@@ -61,7 +61,7 @@ int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, con
     const int Nc = v.Nc;
     P.B = B;
     P.W = W;
-    P.Wp = W <= 4 ? 4 : 8;
+    P.Wp = W;
     P.ntiles = (Nc + B - 1) / B;
     std::vector<int> iperm(Nc);
     for (int i = 0; i < Nc; i++) iperm[perm[i]] = i;
@@ -69,11 +69,6 @@ int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, con
         int k = 0;
         while (k + 1 < (int) bc_first.size() && f >= bc_first[k + 1]) k++;
         return k;
-    };
-    // position of face f in user cell u's face list
-    auto pos_in = [&](int u, int f) {
-        for (int j = cf_off[u]; j < cf_off[u + 1]; j++) if (cf_con[j] == f) return j - cf_off[u];
-        return -1;
     };
     P.foff.assign(P.ntiles + 1, 0);
     P.hoff.assign(P.ntiles + 1, 0);
@@ -108,13 +103,9 @@ int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, con
                     fentry[f] = (int) P.efid.size() - e0;
                     const int iL = iperm[uL], iR = iperm[uR];
                     const int la = local(iL), lb = local(iR);
-                    const bool inL = la < B && !ghost[uL], inR = lb < B && !ghost[uR];
-                    short m[8] = {(short) la, (short) lb,
-                                  (short) (inL ? la * W + pos_in(uL, f) : -1),
-                                  (short) (inR ? lb * W + pos_in(uR, f) : -1),
-                                  (short) (f >= F_BC ? bc_of(f) : -1), 0, 0, 0};
+                    short m[4] = {(short) la, (short) lb, (short) (f >= F_BC ? bc_of(f) : -1), 0};
                     P.efid.push_back(f);
-                    P.meta.insert(P.meta.end(), m, m + 8);
+                    P.meta.insert(P.meta.end(), m, m + 4);
                 }
                 const int e = fentry[f];
                 if (e > 16383) return fail(HCFD_EINVAL, "tile plan: too many faces in one tile");
@@ -123,9 +114,9 @@ int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, con
         }
         // pad the entries to a multiple of 4 so every per-tile block is a multiple of 16 B
         while (((int) P.efid.size() - e0) % 4) {
-            short m[8] = {0, 0, -1, -1, -1, 0, 0, 0};
+            short m[4] = {0, 0, -1, 0};
             P.efid.push_back(-1);
-            P.meta.insert(P.meta.end(), m, m + 8);
+            P.meta.insert(P.meta.end(), m, m + 4);
         }
         P.foff[t + 1] = (int) P.efid.size();
         P.hoff[t + 1] = (int) P.halo.size();
@@ -174,38 +165,38 @@ extern "C" int hcfd_plan_check(const hcfd_mesh_view* v, int tile, int keep_numbe
     if (P.foff[0] != 0 || P.foff[P.ntiles] != E || P.hoff[0] != 0 || P.hoff[P.ntiles] != (int) P.halo.size())
         return bad("offset arrays do not span", -1);
     long long cut = 0, internal = 0;
-    std::vector<int> written(B * W);
+    std::vector<int> seen(2 * (size_t) P.Fmax);
     for (int t = 0; t < P.ntiles; t++) {
         const int base = t * B, nb = std::min(B, Nc - base);
         const int f0 = P.foff[t], nf = P.foff[t + 1] - f0, h0 = P.hoff[t], nh = P.hoff[t + 1] - h0;
         if (nf < 0 || nh < 0 || nf % 4 || nf > P.Fmax || nh > P.Hmax) return bad("entry or halo count", t);
         // bulk-copy sizes and offsets: multiples of 16 bytes (float and double layouts)
-        if ((nb * 16) % 16 || (f0 * 32) % 16 || (f0 * 16) % 16 || (base * 16) % 16) return bad("bulk alignment", t);
+        if ((f0 * 8) % 16 || (base * P.Wp * 2) % 16 || (B * P.Wp * 2) % 16) return bad("bulk alignment", t);
         for (int h = 0; h < nh; h++) {
             const int ci = P.halo[h0 + h];
             if (ci < 0 || ci >= Nc || (ci >= base && ci < base + nb)) return bad("halo id", t);
         }
         auto cell_of = [&](int l) { return l < B ? base + l : P.halo[h0 + l - B]; };
-        std::fill(written.begin(), written.end(), 0);
+        std::fill(seen.begin(), seen.end(), 0);
         for (int e = 0; e < nf; e++) {
-            const short* m = &P.meta[8 * (size_t) (f0 + e)];
-            const int la = m[0], lb = m[1], sL = m[2], sR = m[3], bc = m[4];
+            const short* m = &P.meta[4 * (size_t) (f0 + e)];
+            const int la = m[0], lb = m[1], bc = m[2];
             const int f = P.efid[f0 + e];
             const bool okl = (la < nb) || (la >= B && la < B + nh);
             const bool okr = (lb < nb) || (lb >= B && lb < B + nh);
             if (la < 0 || lb < 0 || !okl || !okr) return bad("local cell index", t);
             if (f < 0) {
-                if (sL != -1 || sR != -1) return bad("padding entry feeds a slot", t);
+                if (bc != -1) return bad("padding entry with a boundary index", t);
                 continue;
             }
             if (cell_of(la) != iperm[v->fc_con[2 * f]] || cell_of(lb) != iperm[v->fc_con[2 * f + 1]])
                 return bad("entry cells differ from the face's cells", t);
             if ((f >= F_BC) != (bc >= 0) || bc >= (int) bc_first.size()) return bad("boundary index", t);
-            if (sL < -1 || sL >= nb * W || sR < -1 || sR >= nb * W) return bad("slot range", t);
-            if (sL >= 0) { if (sL / W != la) return bad("left slot owner", t); written[sL]++; }
-            if (sR >= 0) { if (sR / W != lb) return bad("right slot owner", t); written[sR]++; }
-            if (sL >= 0 && sR >= 0) internal++; else cut++;
+            const bool inL = la < B && !ghost[perm[base + la]], inR = lb < B && !ghost[perm[base + lb]];
+            if (inL && inR) internal++; else cut++;
         }
+        // every real tile cell lists exactly its faces, in increasing face order, each entry
+        // on the side the entry records; every side of an entry is listed by its tile cell
         for (int c = 0; c < nb; c++) {
             const int u = perm[base + c];
             const short* cs = &P.cslot[((size_t) t * B + c) * P.Wp];
@@ -213,17 +204,24 @@ extern "C" int hcfd_plan_check(const hcfd_mesh_view* v, int tile, int keep_numbe
             for (int k = 0; k < P.Wp; k++) {
                 if (k >= deg) {
                     if (cs[k] != -1) return bad("slot beyond the cell's faces", t);
-                    if (k < W && written[c * W + k]) return bad("unused slot written", t);
                     continue;
                 }
                 if (cs[k] < 0) return bad("missing slot", t);
                 const int e = cs[k] >> 1, side = cs[k] & 1;
                 if (e >= nf) return bad("slot entry out of range", t);
-                const short* m = &P.meta[8 * (size_t) (f0 + e)];
+                const short* m = &P.meta[4 * (size_t) (f0 + e)];
                 if ((side ? m[1] : m[0]) != c) return bad("slot side", t);
-                if ((side ? m[3] : m[2]) != c * W + k) return bad("slot position", t);
                 if (P.efid[f0 + e] != cf_con[cf_off[u] + k]) return bad("slot face order", t);
-                if (written[c * W + k] != 1) return bad("slot not written exactly once", t);
+                if (seen[2 * e + side]++) return bad("entry side listed twice", t);
+            }
+        }
+        for (int e = 0; e < nf; e++) {
+            const short* m = &P.meta[4 * (size_t) (f0 + e)];
+            if (P.efid[f0 + e] < 0) continue;
+            for (int side = 0; side < 2; side++) {
+                const int l = m[side];
+                const bool real_in_tile = l < nb && !ghost[perm[base + l]];
+                if (real_in_tile != (seen[2 * e + side] == 1)) return bad("entry side not listed by its cell", t);
             }
         }
     }

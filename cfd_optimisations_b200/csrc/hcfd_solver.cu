@@ -406,7 +406,7 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         return bail(rc);
     }
     if (h->tiled) {
-        if ((rc = dalloc((char**) &h->d_tgeo, tsz * 8 * E)) || (rc = dalloc(&h->d_tmeta, 8 * E)) ||
+        if ((rc = dalloc((char**) &h->d_tgeo, tsz * 8 * E)) || (rc = dalloc(&h->d_tmeta, 4 * E)) ||
             (rc = dalloc(&h->d_foff, h->plan.foff.size())) || (rc = dalloc(&h->d_hoff, h->plan.hoff.size())) ||
             (rc = dalloc(&h->d_halo, h->plan.halo.size())) || (rc = dalloc(&h->d_cslot, h->plan.cslot.size())) ||
             (rc = dalloc(&d_efid, E))) {

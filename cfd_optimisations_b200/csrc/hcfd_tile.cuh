@@ -6,9 +6,9 @@
 //
 // pass 1 (thread per tile cell): Green-Gauss gradient, limiter, CFL dt -> phiG (global).
 // pass 2: face phase (thread per face entry) computes each face flux once per tile and
-//         writes (A_f, F) into the flux slot of each tile cell the face borders; cell phase
-//         (thread per tile cell) sums its slots in increasing face order, updates the cell
-//         and refreshes its ghost cells.
+//         writes F over the staged face record's If/rL/rRx components (the cell phase does
+//         not read them); cell phase (thread per tile cell) sums A_f F of its faces in
+//         increasing face order, updates the cell and refreshes its ghost cells.
 // The arithmetic is that of the thread-per-cell kernels in hcfd_kernels.cuh, operation for
 // operation; only where the operands come from differs.
 #pragma once
@@ -20,11 +20,11 @@ template <class T>
 struct TileArgs {
     StepArgs<T> s;                         // state, stats, BC table, modes
     const T* __restrict__ tgeo;            // face records, per tile component-major: [8][nf]
-    const short* __restrict__ tmeta;       // 8 shorts per entry: la, lb, slotL, slotR, bc, 0, 0, 0
+    const short* __restrict__ tmeta;       // 4 shorts per entry: la, lb, bc, 0
     const int* __restrict__ foff;          // [ntiles + 1], multiples of 4
     const int* __restrict__ hoff;          // [ntiles + 1]
     const int* __restrict__ halo;          // internal cell ids
-    const short* __restrict__ cslot;       // [ntiles * B * Wp]: (entry << 1) | cell-is-right, or -1
+    const short* __restrict__ cslot;       // [ntiles * B * Wp]: (entry << 1) | cell-is-right, or -1; Wp = W
     int ntiles, B, Wp, Hmax, Fmax;
     unsigned int* err;                     // bit 0: a bounded wait gave up
     int ps;                                // plane stride of the cell planes (Nc, or the arena's capacity)
@@ -129,26 +129,33 @@ __device__ __forceinline__ void lds_geo(const T* p, int nf, int e, FaceGeo<T>& g
     g.rLx = p[4 * nf + e]; g.rLy = p[5 * nf + e]; g.rRx = p[6 * nf + e]; g.rRy = p[7 * nf + e];
 }
 
+// Normal and length only (the components pass 2's flux write leaves intact).
+template <class T>
+__device__ __forceinline__ void lds_geo3(const T* p, int nf, int e, T& nx, T& ny, T& Af) {
+    nx = p[e]; ny = p[nf + e]; Af = p[2 * nf + e];
+}
+
 __host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~size_t(127); }
 
-// Shared-memory layout of one CTA: two mbarriers, two staging buffers (double buffering:
-// tile i+1 is in flight while tile i is computed) and, for pass 2, one flux-slot scratch.
-// One staging buffer holds the tile's and its halo's cells (and limited gradients in
-// pass 2), its face records and metadata, its slot table and its iv.
+// Shared-memory layout of one CTA: two mbarriers and two staging buffers (double buffering:
+// tile i+1 is in flight while tile i is computed).  One staging buffer holds the tile's and
+// its halo's cells (and limited gradients in pass 2), its face records and metadata, its
+// slot table and its iv.  Pass 2 keeps its fluxes in the staged face records, so a CTA
+// needs no other scratch (three CTAs of 128 + 32 threads fit an SM at 128-cell tiles).
 template <class T>
 struct TileSmem {
-    size_t u, g, geo, meta, cslot, iv, stage, flux, total;   // byte offsets within a stage
+    size_t u, g, geo, meta, cslot, iv, stage, total;   // byte offsets within a stage
     __host__ __device__ TileSmem(int B, int Hmax, int Fmax, int W, int Wp, bool pass2) {
         size_t p = 0;
         u = p;     p += align128((size_t) (B + Hmax) * sizeof(Cell4<T>));
         g = p;     if (pass2) p += align128((size_t) (B + Hmax) * sizeof(Grad8<T>));
         geo = p;   p += align128((size_t) Fmax * sizeof(FaceGeo<T>));
-        meta = p;  p += align128((size_t) Fmax * 16);
+        meta = p;  p += align128((size_t) Fmax * 8);
         cslot = p; p += align128((size_t) B * Wp * sizeof(short));
         iv = p;    p += align128((size_t) B * sizeof(T));
         stage = p;
-        flux = 128 + 2 * stage;
-        total = flux + (pass2 ? align128((size_t) 5 * B * W * sizeof(T)) : 0);
+        total = 128 + 2 * stage;
+        (void) W;
     }
 };
 
@@ -188,7 +195,7 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
         Grad8<T>* sG = reinterpret_cast<Grad8<T>*>(st + L.g);
         if (lane == 0) {
             const unsigned bu = nb * sizeof(Cell4<T>), bg = PASS2 ? nb * sizeof(Grad8<T>) : 0u;
-            const unsigned bf = nf * sizeof(FaceGeo<T>), bm = nf * 16u;
+            const unsigned bf = nf * sizeof(FaceGeo<T>), bm = nf * 8u;
             const unsigned bs = a.B * a.Wp * sizeof(short), bi = a.B * sizeof(T);
             // the tile's entry count, for the consumers' component-major indexing; published
             // by the release of the arrive below
@@ -208,7 +215,7 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
             }
             if (bf) {
                 bulk_g2s(st + L.geo, a.tgeo + (size_t) f0 * 8, bf, full + buf);
-                bulk_g2s(st + L.meta, a.tmeta + (size_t) f0 * 8, bm, full + buf);
+                bulk_g2s(st + L.meta, a.tmeta + (size_t) f0 * 4, bm, full + buf);
             }
             bulk_g2s(st + L.cslot, a.cslot + (size_t) base * a.Wp, bs, full + buf);
             bulk_g2s(st + L.iv, a.s.iv + base, bi, full + buf);
@@ -279,7 +286,10 @@ __device__ __forceinline__ void finish_step(const StepArgs<T>& a, double r2, int
 // ---------------------------------------------------------------------------------------
 
 __device__ __forceinline__ void lds_slots(const short* p, int Wp, short cs[8]) {
-    if (Wp == 4) {
+    if (Wp == 3) {
+        cs[0] = p[0]; cs[1] = p[1]; cs[2] = p[2];
+        cs[3] = cs[4] = cs[5] = cs[6] = cs[7] = -1;
+    } else if (Wp == 4) {
         const short4 a = *reinterpret_cast<const short4*>(p);
         cs[0] = a.x; cs[1] = a.y; cs[2] = a.z; cs[3] = a.w;
         cs[4] = cs[5] = cs[6] = cs[7] = -1;
@@ -296,16 +306,16 @@ __device__ __forceinline__ void lds_slots(const short* p, int Wp, short cs[8]) {
 // L -> R orientation.  Only the reconstructed states stay live between load and flux.
 template <class T>
 struct FaceIn {
-    T uoL[4], uqR[4], nx, ny, Af;
-    int sL, sR;
+    T uoL[4], uqR[4], nx, ny;
+    int e;
     __device__ __forceinline__ void load(const Cell4<T>* sU, const Grad8<T>* sG, int NL, const T* sGeo,
-                                         const short* sMeta, int nf, int e) {
-        const short4 m = *reinterpret_cast<const short4*>(sMeta + 8 * e);
-        sL = m.z; sR = m.w;
-        const int bc = sMeta[8 * e + 4];
+                                         const short* sMeta, int nf, int e_) {
+        e = e_;
+        const short4 m = *reinterpret_cast<const short4*>(sMeta + 4 * e);
+        const int bc = m.z;
         FaceGeo<T> g;
         lds_geo(sGeo, nf, e, g);
-        nx = g.nx; ny = g.ny; Af = g.Af;
+        nx = g.nx; ny = g.ny;
         T uL[4], uR[4], gL[8];
         lds_cell(sU, NL, m.x, uL);
         lds_cell(sU, NL, m.y, uR);
@@ -330,17 +340,11 @@ struct FaceIn {
         }
     }
     __device__ __forceinline__ void flux(T gma, T F[4]) const { rusanov(uoL, uqR, nx, ny, gma, F); }
-    __device__ __forceinline__ void store(T* sF, int BW, const T F[4]) const {
-        if (sL >= 0) {
-            sF[sL] = Af;
+    // F over components 3..6 (If, rLx, rLy, rRx) of this entry's staged record: only this
+    // thread reads them in pass 2, and it has read them already.
+    __device__ __forceinline__ void store(T* sGeo, int nf, const T F[4]) const {
 #pragma unroll
-            for (int v = 0; v < 4; v++) sF[(v + 1) * BW + sL] = F[v];
-        }
-        if (sR >= 0) {
-            sF[sR] = Af;
-#pragma unroll
-            for (int v = 0; v < 4; v++) sF[(v + 1) * BW + sR] = F[v];
-        }
+        for (int v = 0; v < 4; v++) sGeo[(3 + v) * nf + e] = F[v];
     }
 };
 
@@ -410,7 +414,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
             const bool isL = (cs[k] & 1) == 0;
             FaceGeo<T> g;
             lds_geo(sGeo, nfl, e, g);
-            const int nbl = isL ? sMeta[8 * e + 1] : sMeta[8 * e];
+            const int nbl = isL ? sMeta[4 * e + 1] : sMeta[4 * e];
             T un[4];
             lds_cell(sU, NL, nbl, un);
 #pragma unroll
@@ -495,8 +499,6 @@ __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const TileSmem<T> L(a.B, a.Hmax, a.Fmax, W, a.Wp, true);
     const StepArgs<T>& s = a.s;
-    T* sF = reinterpret_cast<T*>(smem + L.flux);     // [5][B * W]: Af, F0..F3
-    const int BW = a.B * W;
     double dt_used = (s.time_mode == TM_FIXED) ? s.dt_or_cfl
                                                 : s.dt_or_cfl * __longlong_as_double((long long) *s.dtmin);
     double r2 = 0.0;
@@ -523,8 +525,9 @@ __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
         T FA[4], FB[4];
         A.flux(s.gma, FA);
         Bq.flux(s.gma, FB);
-        A.store(sF, BW, FA);
-        if (eB != e) Bq.store(sF, BW, FB);
+        T* sGeoW = reinterpret_cast<T*>(st + L.geo);
+        A.store(sGeoW, nf, FA);
+        if (eB != e) Bq.store(sGeoW, nf, FB);
     }
     compute_sync(NT);
     // cell phase: slots in increasing face order, update, ghost refresh
@@ -544,11 +547,12 @@ __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
         for (int k = 0; k < W; k++) {
             if (cs[k] < 0) continue;
             const bool isL = (cs[k] & 1) == 0;
-            const int sl = c * W + k;
-            const T Af = sF[sl];
+            const int e = cs[k] >> 1;
+            T gnx, gny, Af;
+            lds_geo3(sGeo, nf, e, gnx, gny, Af);
 #pragma unroll
             for (int v = 0; v < 4; v++) {                        // Flux.cpp:39-42
-                const T Fv = sF[(v + 1) * BW + sl];
+                const T Fv = sGeo[(3 + v) * nf + e];
                 if constexpr (COMP) {
                     const T x = isL ? -(Af * Fv) : Af * Fv;
                     two_sum(R[v], Rc[v], x);
@@ -559,7 +563,7 @@ __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
             }
             if (s.time_mode == TM_LOCAL) {
                 FaceGeo<T> g;
-                lds_geo(sGeo, nfl, cs[k] >> 1, g);
+                g.nx = gnx; g.ny = gny; g.Af = Af;
                 lam += wave(cu, cv, ca, g);
             }
         }
@@ -581,15 +585,15 @@ __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
         for (int k = 0; k < W; k++) {
             if (cs[k] < 0 || (cs[k] & 1)) continue;
             const int e = cs[k] >> 1;
-            const int bc = sMeta[8 * e + 4];
+            const int bc = sMeta[4 * e + 2];
             if (bc < 0) continue;
-            const int lb = sMeta[8 * e + 1];
+            const int lb = sMeta[4 * e + 1];
             const int gi = lb < a.B ? base + lb : __ldg(a.halo + h0t + lb - a.B);
-            FaceGeo<T> g;
-            lds_geo(sGeo, nfl, e, g);
+            T gnx, gny, gA;
+            lds_geo3(sGeo, nf, e, gnx, gny, gA);
             T ug[4];
             const BCTable* bt = ARENA ? a.inst_bc + inst : &s.bc;
-            ghost_state(bt->type[bc], un_, g.nx, g.ny, s.gma, bt->UBC[bc], bt->QBC[bc], ug);
+            ghost_state(bt->type[bc], un_, gnx, gny, s.gma, bt->UBC[bc], bt->QBC[bc], ug);
             st_cell(s.Unew, a.ps, gi, ug);
         }
     }
@@ -601,8 +605,8 @@ __global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
         r2 = 0.0;
         bad = 0;
     }
-    compute_sync(NT);   // the next tile's face phase overwrites the flux slots
     if constexpr (ARENA) {
+        compute_sync(NT);   // every warp's tile partial is in s_wr2 / s_wbad
         if (threadIdx.x == 0) {
             double tot = 0.0;
             int b = 0;

@@ -111,6 +111,11 @@ _SIGS = {
                                      ct.c_void_p, _dp, _dp]),
     "hcfd_arena_create": (ct.c_int, [ct.POINTER(ArenaParams), ct.POINTER(ct.c_void_p)]),
     "hcfd_arena_admit": (ct.c_int, [ct.c_void_p, ct.POINTER(MeshView), _ip, ct.c_int, _dp, _dp, ct.c_double, _ip]),
+    "hcfd_arena_prepare": (ct.c_int, [ct.c_void_p, ct.POINTER(MeshView), _ip, ct.c_int, _dp, _dp, ct.c_double,
+                                      ct.POINTER(ct.c_void_p)]),
+    "hcfd_arena_admit_prepared": (ct.c_int, [ct.c_void_p, ct.c_void_p, _ip]),
+    "hcfd_admission_cells": (ct.c_size_t, [ct.c_void_p]),
+    "hcfd_admission_free": (None, [ct.c_void_p]),
     "hcfd_arena_step": (ct.c_int, [ct.c_void_p, ct.c_int]),
     "hcfd_arena_poll": (ct.c_int, [ct.c_void_p, ct.c_int, _ip, ct.POINTER(StepStats), _ip]),
     "hcfd_arena_fetch": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(_dp)]),

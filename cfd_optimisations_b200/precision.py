@@ -24,6 +24,7 @@ import numpy as np
 
 from . import (FP32, FP64, GLOBAL_CFL, LIMITER_BJ, LIMITER_VENKAT, LOCAL_CFL, NUMBER_RANDOM, Mesh, Solver,
                wedge_case)
+from .native import ENONFINITE, HcfdError
 
 LOWER_WALL = 2   # colour of the lower wall (the ramp) in the generated wedge
 
@@ -40,18 +41,30 @@ def converge(mesh: Mesh, precision: int, mach: float, cfl: float, orders: float,
     st = s.step(1, mode, cfl)
     steps += 1
     res0 = st["res_first"]
+    diverged = False
     while steps < max_steps:
         n = min(chunk, max_steps - steps)
-        ms += s.step_timed(n, mode, cfl)
+        try:
+            ms += s.step_timed(n, mode, cfl)
+        except HcfdError as e:
+            if e.code != ENONFINITE:
+                raise
+            diverged = True
         steps += n
+        if diverged:
+            st = dict(res_l2=None, nonfinite=True)
+            break
         st = s.stats()
         hist.append((steps, st["res_l2"]))
-        if st["nonfinite"] or st["res_l2"] <= res0 * 10.0 ** (-orders):
+        if st["res_l2"] <= res0 * 10.0 ** (-orders):
             break
     rho, p = q[0], q[3]
     speed = float(np.hypot(q[1], q[2]))
-    return dict(U=s.U(), cp=s.wall_cp(LOWER_WALL, rho, p, speed), steps=steps, ms=ms, res0=res0,
-                res=st["res_l2"], drop=float(np.log10(res0 / st["res_l2"])) if st["res_l2"] > 0 else None,
+    U = cp = None
+    if not diverged:
+        U, cp = s.U(), s.wall_cp(LOWER_WALL, rho, p, speed)
+    return dict(U=U, cp=cp, steps=steps, ms=ms, res0=res0, diverged=diverged,
+                res=st["res_l2"], drop=float(np.log10(res0 / st["res_l2"])) if st["res_l2"] else None,
                 history=hist)
 
 
@@ -79,9 +92,10 @@ def study(nx=1025, ny=513, mach=3.0, theta=20.0, cfl=0.8, orders=8.0, max_steps=
         runs[name] = converge(mesh, prec, mach, cfl, orders, max_steps, mode=mode, limiter=limiter, K=K,
                               freeze=freeze)
         r = runs[name]
-        out[name] = dict(steps=r["steps"], device_ms=r["ms"], wall_s=time.perf_counter() - t0,
+        out[name] = dict(steps=r["steps"], device_ms=r["ms"], wall_s=time.perf_counter() - t0, diverged=r["diverged"],
                          residual_drop_orders=r["drop"], converged=bool(r["drop"] is not None and r["drop"] >= orders))
-    out["fp32_vs_fp64"] = errors(runs["fp32"], runs["fp64"])
+    out["fp32_vs_fp64"] = (errors(runs["fp32"], runs["fp64"]) if runs["fp32"]["U"] is not None and
+                           runs["fp64"]["U"] is not None else None)
     return out
 
 

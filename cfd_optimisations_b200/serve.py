@@ -1,0 +1,301 @@
+"""Serving loop: wedge-solve requests admitted into one resident arena as they arrive
+(continuous batching), against the plain one-mesh-at-a-time FP64 GPU loop on the same stream.
+
+    python -m cfd_optimisations_b200.serve [--requests 10000 --rate 100 --seed 7 --budget-gb 160
+                                            --orders 6 --max-steps 20000 --chunk 100
+                                            --baseline-sample 24]
+
+Requests arrive as a Poisson process (`rate` per second).  Each carries a wedge: triangle count
+lognormal (median 50,000, sigma 1.0) clipped to [5,000, 2,000,000] on a 2:1 node grid, Mach
+number ~ U[1.8, 4.0], ramp angle ~ U[5, 15] degrees, its own jitter/permutation seed.  A
+request is done when its L2 density residual has dropped `orders` orders below its first value
+or after `max-steps` steps (or when a step produced a NaN/Inf, reported as failed).
+
+The server: worker threads build each arrived request's mesh and prepare its admission (tile
+plan, BC table: hcfd_arena_prepare) while the server thread steps the arena.  Between chunks of
+`chunk` steps the server polls every instance's residual, retires the finished ones (state
+copied to the host, ranges freed) and admits prepared requests, oldest first, as long as the
+HBM budget has room: the batch is never drained.  Admissions and checks happen only between
+chunks, so an instance is checked after the same numbers of its own steps alone and in any
+mix, and its arithmetic does not depend on its neighbours: its result is the same alone and in
+the mix.  Latency is result time minus arrival time, mesh construction included.
+
+The baseline runs each request alone through the plain FP64 solver (Solver, one mesh at a
+time, the same stopping rule checked every `chunk` steps).  Timing it over the whole stream
+would take hours; it is run on `baseline-sample` requests (every k-th request in arrival
+order) and the stream's sequential service time is estimated from them per cell-step, stated
+in the output.  The same sample gives the served results' errors against FP64.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import FP32, FP64, GLOBAL_CFL, KERNEL_CELL, LIMITER_BJ, NUMBER_RANDOM, Mesh, Solver, wedge_case
+
+
+@dataclass
+class Request:
+    rid: int
+    t_arrive: float
+    nx: int
+    ny: int
+    mach: float
+    theta: float
+    seed: int
+
+    @property
+    def triangles(self) -> int:
+        return 2 * (self.nx - 1) * (self.ny - 1)
+
+
+@dataclass
+class Result:
+    rid: int
+    t_arrive: float
+    t_admit: float
+    t_done: float
+    steps: int
+    drop: float
+    converged: bool
+    failed: bool
+    triangles: int
+    U: np.ndarray | None = field(default=None, repr=False)
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_arrive
+
+
+def request_stream(n: int = 10000, rate: float = 100.0, seed: int = 7, median: float = 5e4, sigma: float = 1.0,
+                   lo: float = 5e3, hi: float = 2e6) -> list[Request]:
+    """The seeded request stream (arrival times in seconds from the start)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    ntri = np.clip(np.exp(math.log(median) + sigma * rng.standard_normal(n)), lo, hi)
+    mach = rng.uniform(1.8, 4.0, n)
+    theta = rng.uniform(5.0, 15.0, n)
+    out = []
+    for i in range(n):
+        ny1 = max(2, int(round(math.sqrt(ntri[i] / 4.0))))
+        out.append(Request(i, float(t[i]), 2 * ny1 + 1, ny1 + 1, float(mach[i]), float(theta[i]), 1234 + i))
+    return out
+
+
+def build_mesh(r: Request) -> Mesh:
+    return Mesh.wedge(r.nx, r.ny, theta_deg=r.theta, seed=r.seed, numbering=NUMBER_RANDOM)
+
+
+def done_reason(st: dict, orders: float, max_steps: int) -> str | None:
+    """Why an instance with these statistics is finished, or None."""
+    if st["nonfinite"]:
+        return "failed"
+    if st["res_first"] > 0 and st["res_l2"] <= st["res_first"] * 10.0 ** (-orders):
+        return "converged"
+    if st["steps"] >= max_steps:
+        return "cap"
+    return None
+
+
+def drop_of(st: dict) -> float:
+    return float(math.log10(st["res_first"] / st["res_l2"])) if st["res_l2"] > 0 and st["res_first"] > 0 else 0.0
+
+
+class Server:
+    """Continuous batching of requests into one arena.
+
+    `arena` is an Arena (or any object with prepare/admit_prepared/step/poll/fetch/release);
+    `mesh_for` builds a request's mesh.  Both are parameters so that the scheduling can be
+    exercised without a GPU."""
+
+    def __init__(self, arena, cfl: float = 0.5, orders: float = 6.0, max_steps: int = 20000, chunk: int = 100,
+                 workers: int = 8, lookahead: int = 64, keep=None, mesh_for=build_mesh, clock=time.perf_counter):
+        if max_steps % chunk:
+            raise ValueError("max_steps must be a multiple of chunk")
+        self.arena = arena
+        self.cfl, self.orders, self.max_steps, self.chunk = cfl, orders, max_steps, chunk
+        self.workers, self.lookahead = workers, lookahead
+        self.keep = keep if keep is not None else (lambda rid: False)
+        self.mesh_for = mesh_for
+        self.clock = clock
+        self.busy_s = 0.0          # wall time with at least one instance on the device
+        self.max_active = 0
+        self.max_cells = 0
+
+    def _prepare(self, r: Request):
+        bcmap, qbc, q = wedge_case(r.mach)
+        return self.arena.prepare(self.mesh_for(r), bcmap, qbc, q, self.cfl)
+
+    def run(self, reqs: list[Request]) -> list[Result]:
+        reqs = sorted(reqs, key=lambda r: r.t_arrive)
+        t0 = self.clock()
+        now = lambda: self.clock() - t0
+        pool = ThreadPoolExecutor(max_workers=self.workers)
+        pending = deque()        # (request, future) in arrival order, not yet admitted
+        active = {}              # slot -> (request, t_admit, cells)
+        results = []
+        nxt = 0
+        cells = 0
+        try:
+            while len(results) < len(reqs):
+                t = now()
+                # hand arrived requests to the workers, at most `lookahead` waiting
+                while nxt < len(reqs) and reqs[nxt].t_arrive <= t and len(pending) < self.lookahead:
+                    pending.append((reqs[nxt], pool.submit(self._prepare, reqs[nxt])))
+                    nxt += 1
+                # admit prepared requests, oldest first, while the budget has room
+                blocked = False
+                for item in list(pending):
+                    r, fut = item
+                    if not fut.done():
+                        continue
+                    adm = fut.result()
+                    slot = self.arena.admit_prepared(adm)
+                    if slot is None:
+                        blocked = True
+                        break
+                    pending.remove(item)
+                    active[slot] = (r, now(), adm.cells)
+                    cells += adm.cells
+                    del adm
+                self.max_active = max(self.max_active, len(active))
+                self.max_cells = max(self.max_cells, cells)
+                if not active:
+                    if blocked:
+                        raise RuntimeError("serve: a request does not fit in an empty arena")
+                    # idle: wait for the next arrival or preparation
+                    waits = [reqs[nxt].t_arrive - now()] if nxt < len(reqs) and len(pending) < self.lookahead else []
+                    time.sleep(min([0.002] + [w for w in waits if w > 0]))
+                    continue
+                tb = now()
+                self.arena.step(self.chunk)
+                stats = self.arena.poll()
+                self.busy_s += now() - tb
+                for slot, st in stats.items():
+                    why = done_reason(st, self.orders, self.max_steps)
+                    if why is None:
+                        continue
+                    r, t_adm, c = active.pop(slot)
+                    U = self.arena.fetch(slot) if self.keep(r.rid) else None
+                    self.arena.release(slot)
+                    cells -= c
+                    results.append(Result(r.rid, r.t_arrive, t_adm, now(), int(st["steps"]), drop_of(st),
+                                          why == "converged", why == "failed", r.triangles, U))
+        finally:
+            pool.shutdown(wait=True, cancel_futures=True)
+        return sorted(results, key=lambda x: x.rid)
+
+
+def solve_alone_fp64(r: Request, cfl: float, orders: float, max_steps: int, chunk: int, **kw):
+    """One request through the plain FP64 solver; returns (device ms, Result-like dict, U)."""
+    bcmap, qbc, q = wedge_case(r.mach)
+    s = Solver(build_mesh(r), precision=FP64, limiter=LIMITER_BJ, **kw)
+    s.gather_bcs(bcmap, qbc)
+    s.initialise(q)
+    ms, steps = 0.0, 0
+    while True:
+        ms += s.step_timed(chunk, GLOBAL_CFL, cfl)
+        steps += chunk
+        st = s.stats()
+        st["steps"] = steps
+        why = done_reason(st, orders, max_steps)
+        if why is not None:
+            return ms, dict(steps=steps, drop=drop_of(st), why=why), s.U()
+
+
+def percentiles(x) -> dict:
+    x = np.asarray(x, dtype=float)
+    return dict(p50=float(np.percentile(x, 50)), p99=float(np.percentile(x, 99)), mean=float(x.mean()))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--requests", type=int, default=10000)
+    ap.add_argument("--rate", type=float, default=100.0)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--budget-gb", type=float, default=160.0)
+    ap.add_argument("--orders", type=float, default=6.0)
+    ap.add_argument("--max-steps", type=int, default=20000)
+    ap.add_argument("--chunk", type=int, default=100)
+    ap.add_argument("--cfl", type=float, default=0.5)
+    ap.add_argument("--tile", type=int, default=0, help="arena tile size (0: autotuned for the median request)")
+    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--baseline-sample", type=int, default=24)
+    a = ap.parse_args()
+
+    from . import autotune
+    from .arena import Arena
+    import torch  # noqa: F401  (device memory query only)
+
+    reqs = request_stream(a.requests, a.rate, a.seed)
+    free, total = torch.cuda.mem_get_info()
+    budget = int(min(a.budget_gb * 1e9, free - 4e9))
+    med = int(np.median([r.triangles for r in reqs]))
+    tile = a.tile or autotune.best_arena_tile(med, FP32, LIMITER_BJ)
+    k = max(1, len(reqs) // max(1, a.baseline_sample))
+    sample = set(r.rid for r in reqs[::k][:a.baseline_sample])
+    arena = Arena(budget, precision=FP32, limiter=LIMITER_BJ, time_mode=GLOBAL_CFL, tile=tile,
+                  max_instances=4096)
+    srv = Server(arena, a.cfl, a.orders, a.max_steps, a.chunk, workers=a.workers, keep=lambda rid: rid in sample)
+    t0 = time.perf_counter()
+    res = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    span = max(r.t_done for r in res)
+    lat = [r.latency for r in res]
+    cell_steps = sum(r.triangles * r.steps for r in res)
+    out = dict(
+        workload=dict(requests=a.requests, rate_per_s=a.rate, seed=a.seed, triangles="lognormal median 5e4 sigma 1.0 "
+                      "clipped [5e3, 2e6]", mach="U[1.8,4.0]", theta_deg="U[5,15]", stop=f"{a.orders} orders or "
+                      f"{a.max_steps} steps", chunk=a.chunk, limiter="barth-jespersen", cfl=a.cfl,
+                      time_mode="global per instance"),
+        served=dict(precision="fp32-compensated", tile=tile, budget_bytes=budget, wall_s=wall, makespan_s=span,
+                    solves_per_s=len(res) / span, latency_s=percentiles(lat),
+                    queue_s=percentiles([r.t_admit - r.t_arrive for r in res]),
+                    converged=sum(r.converged for r in res), failed=sum(r.failed for r in res),
+                    steps=percentiles([r.steps for r in res]), cell_updates_per_s=cell_steps / span,
+                    device_busy_fraction=srv.busy_s / span, max_active=srv.max_active, max_cells=srv.max_cells))
+    del arena
+    # baseline on the sample
+    base, errs, errs64 = [], [], []
+    for r in reqs:
+        if r.rid not in sample:
+            continue
+        ms, info, U64 = solve_alone_fp64(r, a.cfl, a.orders, a.max_steps, a.chunk)
+        base.append((r, ms / 1e3, info))
+        served = next(x for x in res if x.rid == r.rid)
+        den = np.abs(U64).max(axis=1)
+        errs.append(dict(rid=r.rid, triangles=r.triangles, steps_fp32=served.steps, steps_fp64=info["steps"],
+                         rel_linf=float((np.abs(served.U - U64).max(axis=1) / den).max())))
+        # the same FP64 solve by the per-cell kernels: it differs from the tiled one only in
+        # the rounding of fused multiply-adds, so this is the spread that rounding alone gives
+        _, info2, U64b = solve_alone_fp64(r, a.cfl, a.orders, a.max_steps, a.chunk, kernel=KERNEL_CELL)
+        errs64.append(float((np.abs(U64b - U64).max(axis=1) / den).max()))
+    per_cell_step = sum(s for _, s, _ in base) / sum(r.triangles * i["steps"] for r, _, i in base)
+    # sequential service of the whole stream, each request's time estimated from its cell-steps
+    by_rid = {x.rid: x for x in res}
+    t_free, lat_b = 0.0, []
+    for r in reqs:
+        svc = per_cell_step * r.triangles * by_rid[r.rid].steps
+        t_free = max(t_free, r.t_arrive) + svc
+        lat_b.append(t_free - r.t_arrive)
+    out["fp64_sequential"] = dict(sample=len(base), sample_device_s=sum(s for _, s, _ in base),
+                                  s_per_cell_step=per_cell_step, estimated_makespan_s=t_free,
+                                  solves_per_s=len(reqs) / t_free, latency_s=percentiles(lat_b),
+                                  note="device time of the sampled requests, extrapolated per cell-step to the "
+                                       "stream (steps per request as served)")
+    out["speedup_solves_per_s"] = out["served"]["solves_per_s"] / out["fp64_sequential"]["solves_per_s"]
+    e32 = [e["rel_linf"] for e in errs]
+    out["fp32_vs_fp64_rel_linf"] = dict(n=len(e32), max=max(e32), median=float(np.median(e32)), per_request=errs)
+    out["fp64_tiled_vs_fp64_cell_rel_linf"] = dict(n=len(errs64), max=max(errs64), median=float(np.median(errs64)))
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

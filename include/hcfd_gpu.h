@@ -253,6 +253,19 @@ int  hcfd_arena_create(const hcfd_arena_params* params, hcfd_arena** out);
  * the budget, a free range or an instance slot is missing: retry after a release. */
 int  hcfd_arena_admit(hcfd_arena* a, const hcfd_mesh_view* mesh, const int* bcmap, int nbcmap, const double* qbc,
                       const double* qic, double dt_or_cfl, int* slot);
+/* The same admission in two halves, so that a server can build tile plans on worker
+ * threads while another thread steps the arena.  hcfd_arena_prepare does the host work
+ * (cell->face table, Morton order, tile plan, BC table); it reads only the arena's fixed
+ * parameters, so any number of threads may call it at once.  The mesh arrays must stay
+ * valid until the admission is freed.  hcfd_arena_admit_prepared claims the ranges, uploads
+ * and activates; on HCFD_EAGAIN the admission stays valid for a later try. */
+typedef struct hcfd_admission hcfd_admission;
+int  hcfd_arena_prepare(const hcfd_arena* a, const hcfd_mesh_view* mesh, const int* bcmap, int nbcmap,
+                        const double* qbc, const double* qic, double dt_or_cfl, hcfd_admission** out);
+int  hcfd_arena_admit_prepared(hcfd_arena* a, const hcfd_admission* adm, int* slot);
+/* Arena cells (whole tiles) the admission will take. */
+size_t hcfd_admission_cells(const hcfd_admission* adm);
+void hcfd_admission_free(hcfd_admission* adm);
 /* Advances every active instance by nsteps steps (enqueued; returns without waiting). */
 int  hcfd_arena_step(hcfd_arena* a, int nsteps);
 /* Waits, then reports up to max active instances: their slots and step statistics. */
