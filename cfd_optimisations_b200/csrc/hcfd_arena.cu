@@ -71,7 +71,7 @@ struct FreeList {
 
 struct Inst {
     bool active = false;
-    int Nc = 0, Nf = 0, Nreal = 0, ntiles = 0;
+    int Nc = 0, Nf = 0, Nreal = 0, ntiles = 0, Hmax = 0, Fmax = 0;
     size_t c0 = 0, ncell = 0, e0 = 0, ne = 0, h0 = 0, nh = 0;
     int* d_perm = nullptr;                 // instance internal -> input cell number
     std::vector<int> tiles;                // 8 ints per tile, arena offsets
@@ -80,20 +80,42 @@ struct Inst {
 };
 
 // Per active instance: its slot and its tile range in the active list.
-__global__ void arena_finalize_kernel(int nact, const int4* __restrict__ act, const double* __restrict__ tile_r2,
-                                      const int* __restrict__ tile_bad, const double* __restrict__ inst_dt,
-                                      unsigned long long* inst_dtmin, hcfd::StepStats* stats, int time_mode, int par) {
+__global__ void __launch_bounds__(512) arena_finalize_kernel(int nact, const int4* __restrict__ act,
+                                                             const double* __restrict__ tile_r2,
+                                                             const int* __restrict__ tile_bad,
+                                                             const double* __restrict__ inst_dt,
+                                                             unsigned long long* inst_dtmin, hcfd::StepStats* stats,
+                                                             int time_mode, int par) {
+    __shared__ double sx[16];
+    __shared__ int sb[16];
     const int i = blockIdx.x;
     if (i >= nact) return;
     const int4 d = act[i];
     const int slot = d.x, t0 = d.y, t1 = d.z;
-    const int lane = threadIdx.x;
-    double x = 0.0;
+    // The instance's tiles are summed in an order fixed relative to its first tile (thread
+    // k takes tiles k, k + 512, ... in four interleaved chains, then the threads in a fixed
+    // tree), so the residual does not depend on where the instance sits in the arena.
+    const int k = threadIdx.x, n = t1 - t0;
+    double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
     int b = 0;
-    for (int t = t0 + lane; t < t1; t += 32) { x += tile_r2[t]; b |= tile_bad[t]; }
-    x = hcfd::warp_sum(x);
+    int j = k;
+    for (; j + 3 * 512 < n; j += 4 * 512) {
+        x0 += tile_r2[t0 + j];
+        x1 += tile_r2[t0 + j + 512];
+        x2 += tile_r2[t0 + j + 1024];
+        x3 += tile_r2[t0 + j + 1536];
+        b |= tile_bad[t0 + j] | tile_bad[t0 + j + 512] | tile_bad[t0 + j + 1024] | tile_bad[t0 + j + 1536];
+    }
+    for (; j < n; j += 512) { x0 += tile_r2[t0 + j]; b |= tile_bad[t0 + j]; }
+    double x = hcfd::warp_sum((x0 + x1) + (x2 + x3));
     b = __any_sync(0xffffffffu, b);
-    if (lane == 0) {
+    const int lane = k & 31, wid = k >> 5;
+    if (lane == 0) { sx[wid] = x; sb[wid] = b; }
+    __syncthreads();
+    if (k == 0) {
+        x = 0.0;
+        b = 0;
+        for (int w = 0; w < (int) (blockDim.x >> 5); w++) { x += sx[w]; b |= sb[w]; }
         hcfd::StepStats* st = stats + slot;
         st->res2_last = x;
         if (st->steps == 0) st->res2_first = x;
@@ -157,7 +179,8 @@ struct hcfd_arena {
     hcfd_arena_params prm{};
     int device = 0, nsm = 0;
     cudaStream_t stream = nullptr;
-    int B = 128, W = 3, Wp = 4, Hcap = 112, Fcap = 288;
+    int B = 128, W = 3, Wp = 4, Hcap = 112, Fcap = 288;   // staging capacities (admission limit)
+    int Hcur = 0, Fcur = 0;                               // largest halo / entries of the active tiles
     size_t Ccap = 0, Ecap = 0, HLcap = 0;
     FreeList fc, fe, fh;
     size_t tsz = 8;
@@ -235,8 +258,8 @@ hcfd::TileArgs<T> arena_args(hcfd_arena* A, int cur, int par) {
     a.ntiles = A->nact_tiles;
     a.B = A->B;
     a.Wp = A->Wp;
-    a.Hmax = A->Hcap;
-    a.Fmax = A->Fcap;
+    a.Hmax = A->Hcur;
+    a.Fmax = A->Fcur;
     a.err = A->err;
     a.ps = (int) A->Ccap;
     a.tiles = A->tiles;
@@ -255,7 +278,7 @@ int enqueue_step(hcfd_arena* A, int cur, int par) {
     constexpr bool COMP = std::is_same<T, float>::value;
     hcfd::tile_pass1_kernel<T, W, true><<<A->grid1, A->B + 32, A->smem1, A->stream>>>(a);
     hcfd::tile_pass2_kernel<T, W, COMP, true><<<A->grid2, A->B + 32, A->smem2, A->stream>>>(a);
-    arena_finalize_kernel<<<A->nact, 32, 0, A->stream>>>(A->nact, A->act, A->tile_r2, A->tile_bad, A->inst_dt,
+    arena_finalize_kernel<<<A->nact, 512, 0, A->stream>>>(A->nact, A->act, A->tile_r2, A->tile_bad, A->inst_dt,
                                                          A->inst_dtmin, A->stats, A->time_mode, par);
     CK(cudaGetLastError());
     return HCFD_OK;
@@ -269,13 +292,26 @@ int enqueue_step_w(hcfd_arena* A, int cur, int par) {
 template <class T, int W>
 int setup_kernels(hcfd_arena* A) {
     constexpr bool COMP = std::is_same<T, float>::value;
-    A->smem1 = hcfd::TileSmem<T>(A->B, A->Hcap, A->Fcap, W, A->Wp, false).total;
-    A->smem2 = hcfd::TileSmem<T>(A->B, A->Hcap, A->Fcap, W, A->Wp, true).total;
+    // the attributes allow the largest staging the arena admits; launches size the shared
+    // memory to the active instances (configure_kernels)
+    const size_t s1 = hcfd::TileSmem<T>(A->B, A->Hcap, A->Fcap, W, A->Wp, false).total;
+    const size_t s2 = hcfd::TileSmem<T>(A->B, A->Hcap, A->Fcap, W, A->Wp, true).total;
     int maxsm = 0;
     CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, A->device));
-    if ((int) A->smem2 > maxsm) return fail(HCFD_EINVAL, "arena: tile does not fit in shared memory");
-    CK(cudaFuncSetAttribute(hcfd::tile_pass1_kernel<T, W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) A->smem1));
-    CK(cudaFuncSetAttribute(hcfd::tile_pass2_kernel<T, W, COMP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) A->smem2));
+    if ((int) s2 > maxsm || (int) s1 > maxsm) return fail(HCFD_EINVAL, "arena: tile does not fit in shared memory");
+    CK(cudaFuncSetAttribute(hcfd::tile_pass1_kernel<T, W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) s1));
+    CK(cudaFuncSetAttribute(hcfd::tile_pass2_kernel<T, W, COMP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) s2));
+    return HCFD_OK;
+}
+
+// Shared memory and persistent grids for the current staging sizes (Hcur, Fcur): staging
+// sized to the active instances rather than to the admission limit lets more CTAs share
+// an SM.
+template <class T, int W>
+int configure_kernels(hcfd_arena* A) {
+    constexpr bool COMP = std::is_same<T, float>::value;
+    A->smem1 = hcfd::TileSmem<T>(A->B, A->Hcur, A->Fcur, W, A->Wp, false).total;
+    A->smem2 = hcfd::TileSmem<T>(A->B, A->Hcur, A->Fcur, W, A->Wp, true).total;
     int b1 = 0, b2 = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, hcfd::tile_pass1_kernel<T, W, true>, A->B + 32, A->smem1));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, hcfd::tile_pass2_kernel<T, W, COMP, true>, A->B + 32, A->smem2));
@@ -285,14 +321,22 @@ int setup_kernels(hcfd_arena* A) {
     return HCFD_OK;
 }
 
+int configure(hcfd_arena* A) {
+    return A->fp32() ? (A->W == 3 ? configure_kernels<float, 3>(A) : configure_kernels<float, 4>(A))
+                     : (A->W == 3 ? configure_kernels<double, 3>(A) : configure_kernels<double, 4>(A));
+}
+
 // Rebuilds the active tile list and the per-instance tile ranges, in slot order.
 int rebuild_active(hcfd_arena* A) {
     std::vector<int> tl;
     std::vector<int4> act;
+    int hmax = 0, fmax = 4;
     for (size_t k = 0; k < A->inst.size(); k++) {
         const Inst& I = A->inst[k];
         if (!I.active) continue;
         const int t0 = (int) (tl.size() / 8);
+        hmax = std::max(hmax, I.Hmax);
+        fmax = std::max(fmax, I.Fmax);
         tl.insert(tl.end(), I.tiles.begin(), I.tiles.end());
         act.push_back(make_int4((int) k, t0, (int) (tl.size() / 8), 0));
     }
@@ -303,7 +347,9 @@ int rebuild_active(hcfd_arena* A) {
     if (!act.empty()) CK(cudaMemcpyAsync(A->act, act.data(), sizeof(int4) * act.size(), cudaMemcpyHostToDevice, A->stream));
     CK(cudaStreamSynchronize(A->stream));
     free_graph(A);
-    return HCFD_OK;
+    A->Hcur = hmax;
+    A->Fcur = fmax;
+    return configure(A);
 }
 
 template <class P>
@@ -478,7 +524,7 @@ int hcfd_arena_admit_prepared(hcfd_arena* A, const hcfd_admission* D, int* slot_
     const int Nc = D->Nc, Nf = D->Nf, F_BC = D->F_BC;
     // ranges in the arena (budget admission)
     Inst I;
-    I.Nc = Nc; I.Nf = Nf; I.Nreal = D->nreal; I.ntiles = P.ntiles;
+    I.Nc = Nc; I.Nf = Nf; I.Nreal = D->nreal; I.ntiles = P.ntiles; I.Hmax = P.Hmax; I.Fmax = P.Fmax;
     I.ncell = (size_t) P.ntiles * A->B;
     I.ne = P.efid.size();
     I.nh = P.halo.size();

@@ -471,12 +471,18 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
         if (s.time_mode != TM_FIXED) dtc = fmin(dtc, (double) (T(1) / (iv * lam)));
     }
     if constexpr (ARENA) {
-        // per-instance minimum: one atomic per warp and tile (min is exact, order-free)
+        // per-instance minimum (exact and order-free): each warp carries its minimum across
+        // this CTA's consecutive tiles of one instance and posts it with one atomic when the
+        // next tile belongs to another instance, so a large instance sees a few atomics per
+        // CTA rather than one per warp and tile on a single address
         if (s.time_mode != TM_FIXED) {
-            const double m = warp_min(dtc);
-            if ((threadIdx.x & 31) == 0 && m < 1e300)
-                atomicMin(a.inst_dtmin + 2 * inst + a.par, (unsigned long long) __double_as_longlong(m));
-            dtc = 1e300;
+            const int tn = t + (int) gridDim.x;
+            if (tn >= a.ntiles || __ldg(&a.tiles[2 * tn].w) != inst) {
+                const double m = warp_min(dtc);
+                if ((threadIdx.x & 31) == 0 && m < 1e300)
+                    atomicMin(a.inst_dtmin + 2 * inst + a.par, (unsigned long long) __double_as_longlong(m));
+                dtc = 1e300;
+            }
         }
     }
     HCFD_TILE_LOOP_END
@@ -495,7 +501,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
 }
 
 template <class T, int W, bool COMP, bool ARENA>
-__global__ void __maxnreg__(112) tile_pass2_kernel(const TileArgs<T> a) {
+__global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const TileSmem<T> L(a.B, a.Hmax, a.Fmax, W, a.Wp, true);
     const StepArgs<T>& s = a.s;
