@@ -125,11 +125,11 @@ class Solver:
 
     def __init__(self, mesh: Mesh, gma: float = 1.4, limiter: int = LIMITER_BJ, venkat_K: float = 5.0,
                  precision: int = FP64, block: int = 0, kernel: int = 0, tile: int = 0,
-                 keep_numbering: bool = False, freeze_limiter_after: int = 0):
+                 keep_numbering: bool = False, freeze_limiter_after: int = 0, tile2: int = 0):
         self._mesh = mesh
         v = mesh.view()
         p = _n.Params(gma, limiter, venkat_K, precision, block, kernel, tile, 1 if keep_numbering else 0,
-                      freeze_limiter_after)
+                      freeze_limiter_after, tile2)
         h = ct.c_void_p()
         _n.check(_n.lib().hcfd_gpu_create(ct.byref(v), ct.byref(p), ct.byref(h)))
         self._h = h

@@ -53,6 +53,19 @@ void prim_to_cons(const double* q, double gma, double* u) {
 
 }  // namespace
 
+// One tile plan of the tiled kernels and its device arrays.  Pass 1 and pass 2 may run on
+// different tilings of the same internal cell order (pass 2, which computes each face flux
+// once per tile, gains from larger tiles than pass 1 does).
+struct TiledPass {
+    hcfd::TilePlan plan;
+    void* d_tgeo = nullptr;              // face records [entries], T
+    short* d_tmeta = nullptr;
+    int *d_foff = nullptr, *d_hoff = nullptr, *d_halo = nullptr;
+    short* d_cslot = nullptr;
+    int* d_efid = nullptr;               // set-up only
+    int block = 0;                       // compute threads per CTA
+};
+
 struct hcfd_solver {
     int device = 0, nsm = 0;
     cudaStream_t stream = nullptr;
@@ -79,11 +92,8 @@ struct hcfd_solver {
     unsigned int* d_err = nullptr;
     hcfd::StepStats* d_stats = nullptr;
     // tiled kernels
-    hcfd::TilePlan plan;
-    void* d_tgeo = nullptr;              // FaceGeo<T> [entries]
-    short* d_tmeta = nullptr;
-    int *d_foff = nullptr, *d_hoff = nullptr, *d_halo = nullptr;
-    short* d_cslot = nullptr;
+    TiledPass tp[2];                     // pass 1; pass 2 when it has its own tiling
+    bool split = false;                  // pass 2 uses tp[1]
     size_t smem1 = 0, smem2 = 0;
     int grid1 = 0, grid2 = 0;
     bool tiled = false;
@@ -108,9 +118,12 @@ void free_all(hcfd_solver* s) {
     for (auto e : s->ev1) cudaEventDestroy(e);
     for (auto e : s->ev2) cudaEventDestroy(e);
     void* ptrs[] = {s->d_fc, s->d_perm, s->d_slot, s->d_geo64, s->d_geoT, s->d_iv, s->d_U[0], s->d_U[1],
-                    s->d_phiG, s->d_phiF, s->d_io, s->d_cp, s->d_dtmin, s->d_partial, s->d_counter, s->d_err, s->d_stats,
-                    s->d_tgeo, s->d_tmeta, s->d_foff, s->d_hoff, s->d_halo, s->d_cslot};
+                    s->d_phiG, s->d_phiF, s->d_io, s->d_cp, s->d_dtmin, s->d_partial, s->d_counter, s->d_err, s->d_stats};
     for (void* p : ptrs) if (p) cudaFree(p);
+    for (TiledPass& P : s->tp) {
+        void* q[] = {P.d_tgeo, P.d_tmeta, P.d_foff, P.d_hoff, P.d_halo, P.d_cslot, P.d_efid};
+        for (void* p : q) if (p) cudaFree(p);
+    }
     if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -142,20 +155,20 @@ hcfd::StepArgs<T> step_args(hcfd_solver* s, int time_mode, double dt_or_cfl) {
 }
 
 template <class T>
-hcfd::TileArgs<T> tile_args(hcfd_solver* s, int time_mode, double dt_or_cfl) {
+hcfd::TileArgs<T> tile_args(hcfd_solver* s, int time_mode, double dt_or_cfl, const TiledPass& P) {
     hcfd::TileArgs<T> a;
     a.s = step_args<T>(s, time_mode, dt_or_cfl);
-    a.tgeo = (const T*) s->d_tgeo;
-    a.tmeta = s->d_tmeta;
-    a.foff = s->d_foff;
-    a.hoff = s->d_hoff;
-    a.halo = s->d_halo;
-    a.cslot = s->d_cslot;
-    a.ntiles = s->plan.ntiles;
-    a.B = s->plan.B;
-    a.Wp = s->plan.Wp;
-    a.Hmax = s->plan.Hmax;
-    a.Fmax = s->plan.Fmax;
+    a.tgeo = (const T*) P.d_tgeo;
+    a.tmeta = P.d_tmeta;
+    a.foff = P.d_foff;
+    a.hoff = P.d_hoff;
+    a.halo = P.d_halo;
+    a.cslot = P.d_cslot;
+    a.ntiles = P.plan.ntiles;
+    a.B = P.plan.B;
+    a.Wp = P.plan.Wp;
+    a.Hmax = P.plan.Hmax;
+    a.Fmax = P.plan.Fmax;
     a.err = s->d_err;
     a.ps = s->Nc;
     a.tiles = nullptr;
@@ -192,12 +205,14 @@ int launch_step(hcfd_solver* s, int time_mode, double dt_or_cfl) {
     Ev e1, e2;
     int rc;
     if (s->tiled) {
-        hcfd::TileArgs<T> a = tile_args<T>(s, time_mode, dt_or_cfl);
+        const TiledPass& P2 = s->split ? s->tp[1] : s->tp[0];
+        const hcfd::TileArgs<T> a1 = tile_args<T>(s, time_mode, dt_or_cfl, s->tp[0]);
+        const hcfd::TileArgs<T> a2 = tile_args<T>(s, time_mode, dt_or_cfl, P2);
         if ((rc = prof_begin(s, e1))) return rc;
-        hcfd::tile_pass1_kernel<T, W, false><<<s->grid1, s->block + 32, s->smem1, s->stream>>>(a);
+        hcfd::tile_pass1_kernel<T, W, false><<<s->grid1, s->tp[0].block + 32, s->smem1, s->stream>>>(a1);
         if ((rc = prof_end(s, e1, s->ev1))) return rc;
         if ((rc = prof_begin(s, e2))) return rc;
-        hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value, false><<<s->grid2, s->block + 32, s->smem2, s->stream>>>(a);
+        hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value, false><<<s->grid2, P2.block + 32, s->smem2, s->stream>>>(a2);
         if ((rc = prof_end(s, e2, s->ev2))) return rc;
     } else {
         const int grid = nblk(s->Nc, s->block);
@@ -226,9 +241,11 @@ int launch_step_w(hcfd_solver* s, int time_mode, double dt_or_cfl) {
 // Shared-memory opt-in and persistent grid size of the tiled kernels for one (T, W).
 template <class T, int W>
 int setup_tiled_w(hcfd_solver* s) {
-    const hcfd::TilePlan& P = s->plan;
+    const hcfd::TilePlan& P = s->tp[0].plan;
+    const TiledPass& T2 = s->split ? s->tp[1] : s->tp[0];
+    const hcfd::TilePlan& Q = T2.plan;
     s->smem1 = hcfd::TileSmem<T>(P.B, P.Hmax, P.Fmax, W, P.Wp, false).total;
-    s->smem2 = hcfd::TileSmem<T>(P.B, P.Hmax, P.Fmax, W, P.Wp, true).total;
+    s->smem2 = hcfd::TileSmem<T>(Q.B, Q.Hmax, Q.Fmax, W, Q.Wp, true).total;
     int maxsm = 0;
     CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
     if ((int) s->smem2 > maxsm || (int) s->smem1 > maxsm) return fail(HCFD_EINVAL, "tile does not fit in shared memory");
@@ -237,12 +254,13 @@ int setup_tiled_w(hcfd_solver* s) {
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int) s->smem2));
     int b1 = 0, b2 = 0;
     // blocks of the tiled kernels: `block` compute threads + one producer warp
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, hcfd::tile_pass1_kernel<T, W, false>, s->block + 32, s->smem1));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, hcfd::tile_pass1_kernel<T, W, false>, s->tp[0].block + 32,
+                                                     s->smem1));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value, false>,
-                                                     s->block + 32, s->smem2));
+                                                     T2.block + 32, s->smem2));
     if (b1 < 1 || b2 < 1) return fail(HCFD_EINVAL, "tiled kernels cannot be resident");
     s->grid1 = std::min(P.ntiles, b1 * s->nsm);
-    s->grid2 = std::min(P.ntiles, b2 * s->nsm);
+    s->grid2 = std::min(Q.ntiles, b2 * s->nsm);
     return HCFD_OK;
 }
 
@@ -298,12 +316,13 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
     *out = nullptr;
     int rc = hcfd::validate_view(*mv);
     if (rc != HCFD_OK) return rc;
-    hcfd_params p{1.4, HCFD_LIMITER_BJ, 5.0, HCFD_FP64, 0, HCFD_KERNEL_TILED, 0, 0, 0};
+    hcfd_params p{1.4, HCFD_LIMITER_BJ, 5.0, HCFD_FP64, 0, HCFD_KERNEL_TILED, 0, 0, 0, 0};
     if (prm) p = *prm;
     if (!(p.gma > 1.0) || (p.limiter != HCFD_LIMITER_BJ && p.limiter != HCFD_LIMITER_VENKAT) ||
         (p.precision != HCFD_FP64 && p.precision != HCFD_FP32) || p.block < 0 || p.block > 1024 || (p.block % 32) ||
         (p.kernel != HCFD_KERNEL_TILED && p.kernel != HCFD_KERNEL_CELL) || p.tile < 0 || p.tile > 512 || (p.tile % 32) ||
-        (p.kernel == HCFD_KERNEL_TILED && p.block > 256) || p.freeze_limiter_after < 0)
+        (p.kernel == HCFD_KERNEL_TILED && p.block > 256) || p.freeze_limiter_after < 0 ||
+        p.tile2 < 0 || p.tile2 > 512 || (p.tile2 % 32))
         return fail(HCFD_EINVAL, "gpu_create: bad parameters");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -345,13 +364,50 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
     for (int col = s->Ncol - s->NBC; col < s->Ncol; col++) bc_first.push_back(s->coloff[col]);
 
     s->tiled = (p.kernel == HCFD_KERNEL_TILED);
-    // tiled kernels: one compute thread per tile cell unless asked otherwise
-    if (s->tiled && !p.block) s->block = std::min(p.tile ? p.tile : 128, 256);
     std::vector<int2> slot;
     if (s->tiled) {
-        rc = hcfd::build_tile_plan(*mv, cf_off, cf_con, ghost, perm, s->F_BC, bc_first, p.tile ? p.tile : 128,
-                                   s->W, s->plan);
-        if (rc != HCFD_OK) return rc;
+        // Pass 1 on tiles of `tile` cells, pass 2 on tiles of `tile2`.  When neither is given:
+        // FP64 224 and 192 cells, FP32 256 and 128 (pass 2's flux work per tile is heavy in
+        // FP64, and fewer tile cuts pay; measured on the B200), falling back to smaller
+        // tiles where a tiling does not fit shared memory (scattered cells, as with
+        // keep_numbering on a shuffled mesh, have large halos).  When only `tile` is given,
+        // both passes use it.  One compute thread per tile cell unless `block` says otherwise.
+        const bool f64 = p.precision == HCFD_FP64;
+        int maxsm = 0;
+        CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
+        auto need = [&](const hcfd::TilePlan& Q, bool pass2) {
+            return f64 ? hcfd::TileSmem<double>(Q.B, Q.Hmax, Q.Fmax, s->W, Q.Wp, pass2).total
+                       : hcfd::TileSmem<float>(Q.B, Q.Hmax, Q.Fmax, s->W, Q.Wp, pass2).total;
+        };
+        std::vector<int> c1 = p.tile ? std::vector<int>{p.tile} : std::vector<int>{f64 ? 224 : 256, 128, 64};
+        std::vector<int> c2 = p.tile2 ? std::vector<int>{p.tile2}
+                                      : p.tile ? std::vector<int>{p.tile} : std::vector<int>{f64 ? 192 : 128, 128, 64};
+        bool ok = false;
+        for (int t : c1) {
+            rc = hcfd::build_tile_plan(*mv, cf_off, cf_con, ghost, perm, s->F_BC, bc_first, t, s->W, s->tp[0].plan);
+            if (rc != HCFD_OK) return rc;
+            if (need(s->tp[0].plan, false) <= (size_t) maxsm) { ok = true; break; }
+        }
+        if (!ok) return fail(HCFD_EINVAL, "tile does not fit in shared memory");
+        const int tile1 = s->tp[0].plan.B;
+        s->tp[0].block = p.block ? p.block : std::min(tile1, 256);
+        ok = false;
+        for (int t : c2) {
+            if (t == tile1) {
+                if (need(s->tp[0].plan, true) <= (size_t) maxsm) { s->split = false; ok = true; break; }
+                continue;
+            }
+            rc = hcfd::build_tile_plan(*mv, cf_off, cf_con, ghost, perm, s->F_BC, bc_first, t, s->W, s->tp[1].plan);
+            if (rc != HCFD_OK) return rc;
+            if (need(s->tp[1].plan, true) <= (size_t) maxsm) {
+                s->split = true;
+                s->tp[1].block = p.block ? p.block : std::min(t, 256);
+                ok = true;
+                break;
+            }
+        }
+        if (!ok) return fail(HCFD_EINVAL, "tile does not fit in shared memory");
+        if (!s->split) s->tp[1] = TiledPass();
     } else {
         // Per-cell kernels: slot-major table {face or ~face, neighbour}, internal numbering.
         slot.assign((size_t) s->W * Nc, make_int2(-1, -1));
@@ -380,17 +436,18 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         h->partial_len = nblk(Nc, h->block);
     }
     int* d_fn = nullptr; int* d_fcu = nullptr; int* d_cnoff = nullptr; int* d_cncon = nullptr;
-    int* d_cfoff = nullptr; int* d_cfcon = nullptr; int* d_efid = nullptr;
+    int* d_cfoff = nullptr; int* d_cfcon = nullptr;
     double* d_nodes = nullptr; double* d_xc = nullptr; double* d_ivu = nullptr;
     auto free_tmp = [&]() {
         cudaStreamSynchronize(h->stream);
-        void* t[] = {d_fn, d_fcu, d_cnoff, d_cncon, d_cfoff, d_cfcon, d_efid, d_nodes, d_xc, d_ivu};
+        void* t[] = {d_fn, d_fcu, d_cnoff, d_cncon, d_cfoff, d_cfcon, d_nodes, d_xc, d_ivu, h->tp[0].d_efid, h->tp[1].d_efid};
         for (void* q : t) if (q) cudaFree(q);
+        h->tp[0].d_efid = h->tp[1].d_efid = nullptr;
     };
     const int ncn = mv->cn_off[Nc];
-    const size_t E = h->plan.efid.size();
     // iv is read one whole tile at a time by the tiled kernels: pad it to full tiles.
-    const size_t niv = h->tiled ? std::max((size_t) Nc, (size_t) h->plan.ntiles * h->plan.B) : (size_t) Nc;
+    size_t niv = Nc;
+    for (const TiledPass& P : h->tp) niv = std::max(niv, (size_t) P.plan.ntiles * P.plan.B);
     if ((rc = dalloc(&h->d_fc, 2 * (size_t) Nf)) || (rc = dalloc(&h->d_perm, Nc)) ||
         (rc = dalloc(&h->d_geo64, Nf)) || (rc = dalloc((char**) &h->d_iv, tsz * niv)) ||
         (rc = dalloc((char**) &h->d_U[0], tsz * 4 * Nc)) || (rc = dalloc((char**) &h->d_U[1], tsz * 4 * Nc)) ||
@@ -406,12 +463,16 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         return bail(rc);
     }
     if (h->tiled) {
-        if ((rc = dalloc((char**) &h->d_tgeo, tsz * 8 * E)) || (rc = dalloc(&h->d_tmeta, 4 * E)) ||
-            (rc = dalloc(&h->d_foff, h->plan.foff.size())) || (rc = dalloc(&h->d_hoff, h->plan.hoff.size())) ||
-            (rc = dalloc(&h->d_halo, h->plan.halo.size())) || (rc = dalloc(&h->d_cslot, h->plan.cslot.size())) ||
-            (rc = dalloc(&d_efid, E))) {
-            free_tmp();
-            return bail(rc);
+        for (int k = 0; k < (h->split ? 2 : 1); k++) {
+            TiledPass& P = h->tp[k];
+            const size_t E = P.plan.efid.size();
+            if ((rc = dalloc((char**) &P.d_tgeo, tsz * 8 * E)) || (rc = dalloc(&P.d_tmeta, 4 * E)) ||
+                (rc = dalloc(&P.d_foff, P.plan.foff.size())) || (rc = dalloc(&P.d_hoff, P.plan.hoff.size())) ||
+                (rc = dalloc(&P.d_halo, P.plan.halo.size())) || (rc = dalloc(&P.d_cslot, P.plan.cslot.size())) ||
+                (rc = dalloc(&P.d_efid, E))) {
+                free_tmp();
+                return bail(rc);
+            }
         }
     } else {
         if ((rc = dalloc(&h->d_slot, slot.size())) || (f32 && (rc = dalloc((char**) &h->d_geoT, tsz * 8 * (size_t) Nf)))) {
@@ -434,13 +495,16 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
     if (ce == cudaSuccess) ce = up(d_cfcon, cf_con.data(), 4 * cf_con.size());
     if (ce == cudaSuccess) ce = up(d_nodes, mv->nodes, 16 * (size_t) h->Nn);
     if (h->tiled) {
-        const hcfd::TilePlan& P = h->plan;
-        if (ce == cudaSuccess) ce = up(h->d_tmeta, P.meta.data(), 2 * P.meta.size());
-        if (ce == cudaSuccess) ce = up(h->d_foff, P.foff.data(), 4 * P.foff.size());
-        if (ce == cudaSuccess) ce = up(h->d_hoff, P.hoff.data(), 4 * P.hoff.size());
-        if (ce == cudaSuccess) ce = up(h->d_halo, P.halo.data(), 4 * P.halo.size());
-        if (ce == cudaSuccess) ce = up(h->d_cslot, P.cslot.data(), 2 * P.cslot.size());
-        if (ce == cudaSuccess) ce = up(d_efid, P.efid.data(), 4 * E);
+        for (int k = 0; k < (h->split ? 2 : 1); k++) {
+            TiledPass& T = h->tp[k];
+            const hcfd::TilePlan& P = T.plan;
+            if (ce == cudaSuccess) ce = up(T.d_tmeta, P.meta.data(), 2 * P.meta.size());
+            if (ce == cudaSuccess) ce = up(T.d_foff, P.foff.data(), 4 * P.foff.size());
+            if (ce == cudaSuccess) ce = up(T.d_hoff, P.hoff.data(), 4 * P.hoff.size());
+            if (ce == cudaSuccess) ce = up(T.d_halo, P.halo.data(), 4 * P.halo.size());
+            if (ce == cudaSuccess) ce = up(T.d_cslot, P.cslot.data(), 2 * P.cslot.size());
+            if (ce == cudaSuccess) ce = up(T.d_efid, P.efid.data(), 4 * P.efid.size());
+        }
     } else {
         if (ce == cudaSuccess) ce = up(h->d_slot, slot.data(), sizeof(int2) * slot.size());
     }
@@ -454,10 +518,12 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         hcfd::permute_kernel<<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_ivu, h->d_perm, d_xc);
         if (f32) hcfd::convert_iv_kernel<float><<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_xc, (float*) h->d_iv);
         else ce = cudaMemcpyAsync(h->d_iv, d_xc, sizeof(double) * Nc, cudaMemcpyDeviceToDevice, st);
-        if (h->tiled && E) {
-            const int nt = h->plan.ntiles;
-            if (f32) hcfd::gather_geo_kernel<float><<<nt, 128, 0, st>>>(nt, h->d_foff, d_efid, h->d_geo64, (float*) h->d_tgeo);
-            else hcfd::gather_geo_kernel<double><<<nt, 128, 0, st>>>(nt, h->d_foff, d_efid, h->d_geo64, (double*) h->d_tgeo);
+        for (int k = 0; h->tiled && k < (h->split ? 2 : 1); k++) {
+            TiledPass& T = h->tp[k];
+            const int nt = T.plan.ntiles;
+            if (T.plan.efid.empty()) continue;
+            if (f32) hcfd::gather_geo_kernel<float><<<nt, 128, 0, st>>>(nt, T.d_foff, T.d_efid, h->d_geo64, (float*) T.d_tgeo);
+            else hcfd::gather_geo_kernel<double><<<nt, 128, 0, st>>>(nt, T.d_foff, T.d_efid, h->d_geo64, (double*) T.d_tgeo);
         }
         if (!h->tiled && f32)
             hcfd::convert_geo_kernel<float><<<nblk(Nf, 256), 256, 0, st>>>(Nf, h->d_geo64, (hcfd::FaceGeo<float>*) h->d_geoT);

@@ -40,7 +40,7 @@ class WedgeSpec(ct.Structure):
 class Params(ct.Structure):
     _fields_ = [("gma", ct.c_double), ("limiter", ct.c_int), ("venkat_K", ct.c_double),
                 ("precision", ct.c_int), ("block", ct.c_int), ("kernel", ct.c_int), ("tile", ct.c_int),
-                ("keep_numbering", ct.c_int), ("freeze_limiter_after", ct.c_longlong)]
+                ("keep_numbering", ct.c_int), ("freeze_limiter_after", ct.c_longlong), ("tile2", ct.c_int)]
 
 
 class StepStats(ct.Structure):

@@ -134,11 +134,15 @@ typedef struct hcfd_params {
                            most 256 for the tiled kernels), 0 = 256 for the per-cell kernels
                            and one thread per tile cell for the tiled kernels               */
     int    kernel;      /* enum hcfd_kernel                                                  */
-    int    tile;        /* cells per tile of the tiled kernels (32..512, multiple of 32), 0 = 128 */
+    int    tile;        /* cells per tile of the tiled kernels (32..512, multiple of 32); 0 = see tile2 */
     int    keep_numbering; /* 1: keep the input cell order on the device instead of the Morton order */
     long long freeze_limiter_after; /* limiter freezing (not in the reference): steps 1..N compute
                            the limiter, later steps reuse step N's limiter values with fresh
                            gradients, counted from hcfd_gpu_initialise; 0 = never        */
+    int    tile2;       /* cells per tile of pass 2 (32..512, multiple of 32); 0 = `tile` when
+                           that is given; with neither given, pass 1 / pass 2 tiles are
+                           224 / 192 cells in FP64 and 256 / 128 in FP32 (smaller where a
+                           tiling does not fit shared memory)                            */
 } hcfd_params;
 
 /* Step kernels.  HCFD_KERNEL_TILED (default): persistent CTAs stage tiles of cells, their
