@@ -63,14 +63,16 @@ def run_arena(meshes, specs, steps, precision=FP32, limiter=LIMITER_BJ, cfl=0.5,
     return a, slots, stats, t_admit, t_run
 
 
-def run_loop(meshes, specs, steps, precision=FP64, limiter=LIMITER_BJ, cfl=0.5):
+def run_loop(meshes, specs, steps, precision=FP64, limiter=LIMITER_BJ, cfl=0.5, rho_scale=1.0):
     ms, t_create, out = 0.0, 0.0, []
     for m, s in zip(meshes, specs):
         bcmap, qbc, q = wedge_case(s["mach"])
         t0 = time.perf_counter()
         sol = Solver(m, precision=precision, limiter=limiter)
         sol.gather_bcs(bcmap, qbc)
-        sol.initialise(q)
+        qi = list(q)
+        qi[0] *= rho_scale
+        sol.initialise(qi)
         t_create += time.perf_counter() - t0
         sol.step(2, GLOBAL_CFL, cfl)
         ms += sol.step_timed(steps - 2, GLOBAL_CFL, cfl)
@@ -109,6 +111,13 @@ def main():
                                 solves_per_s=a.instances / (ms / 1e3))
         out["speedup_solves_per_s"] = out["arena"]["solves_per_s"] / out["fp64_loop"]["solves_per_s"]
         out["fp32_vs_fp64_rel_linf"] = dict(max=max(errs), median=float(np.median(errs)))
+        # the spread that rounding alone gives: FP64 again from an initial density one
+        # rounding step larger, on every 16th instance
+        sub = list(range(0, len(meshes), 16))
+        _, _, U64p = run_loop([meshes[i] for i in sub], [specs[i] for i in sub], a.steps, rho_scale=1.0 + 2.0 ** -52)
+        e64 = [float(np.max(np.abs(up - U64[i]).max(axis=1) / np.abs(U64[i]).max(axis=1))) for i, up in zip(sub, U64p)]
+        out["fp64_vs_fp64_initial_density_plus_one_ulp_rel_linf"] = dict(n=len(e64), max=max(e64),
+                                                                        median=float(np.median(e64)))
     print(json.dumps(out))
 
 

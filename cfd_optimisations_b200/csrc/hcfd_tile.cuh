@@ -56,6 +56,20 @@ __device__ __forceinline__ void tile_info(const TileArgs<T>& a, int t, int& base
     }
 }
 
+// What the compute warps need of a tile besides its data, written by the producer into the
+// stage header with the tile's copies (published by the same mbarrier), so that the compute
+// warps start a tile without dependent global loads: its descriptor, and for its instance
+// the step count (limiter freezing), the dt or CFL number and the dt minimum of this step.
+struct StageInfo {
+    int base, nb, f0, nf, h0, nh, inst, pad;
+    double dt_or_cfl;
+    double dtmin;
+    long long steps;
+    long long pad2;
+};
+static_assert(sizeof(StageInfo) == 64, "stage info is 64 bytes");
+constexpr int kHeader = 256;   // full[4], empty[4] mbarriers, then StageInfo per stage (two)
+
 // ---------------------------------------------------------------------------------------
 // PTX helpers (sm_90+ bulk copies and mbarriers; sm_80+ cp.async)
 
@@ -154,7 +168,7 @@ struct TileSmem {
         cslot = p; p += align128((size_t) B * Wp * sizeof(short));
         iv = p;    p += align128((size_t) B * sizeof(T));
         stage = p;
-        total = 128 + 2 * stage;
+        total = kHeader + 2 * stage;
         (void) W;
     }
 };
@@ -188,7 +202,7 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
     for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {
         const int buf = iter & 1;
         if (iter >= 2) mbar_wait(empty + buf, ((iter >> 1) - 1) & 1, a.err);
-        unsigned char* st = smem + 128 + buf * L.stage;
+        unsigned char* st = smem + kHeader + buf * L.stage;
         int base, nb, f0, nf, h0, nh, inst;
         tile_info<ARENA>(a, t, base, nb, f0, nf, h0, nh, inst);
         Cell4<T>* sU = reinterpret_cast<Cell4<T>*>(st + L.u);
@@ -197,9 +211,19 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
             const unsigned bu = nb * sizeof(Cell4<T>), bg = PASS2 ? nb * sizeof(Grad8<T>) : 0u;
             const unsigned bf = nf * sizeof(FaceGeo<T>), bm = nf * 8u;
             const unsigned bs = a.B * a.Wp * sizeof(short), bi = a.B * sizeof(T);
-            // the tile's entry count, for the consumers' component-major indexing; published
-            // by the release of the arrive below
-            reinterpret_cast<int*>(smem + 64)[buf] = nf;
+            // the tile's descriptor and instance scalars, published by the release of the
+            // arrive below
+            StageInfo* si = reinterpret_cast<StageInfo*>(smem + 64) + buf;
+            si->base = base; si->nb = nb; si->f0 = f0; si->nf = nf; si->h0 = h0; si->nh = nh; si->inst = inst;
+            if constexpr (ARENA) {
+                si->dt_or_cfl = __ldg(a.inst_dt + inst);
+                si->dtmin = __longlong_as_double((long long) a.inst_dtmin[2 * inst + a.par]);
+                si->steps = a.inst_stats[inst].steps;
+            } else {
+                si->dt_or_cfl = a.s.dt_or_cfl;
+                si->dtmin = __longlong_as_double((long long) *a.s.dtmin);
+                si->steps = a.s.stats->steps;
+            }
             mbar_arrive_expect_tx(full + buf, bu + bg + bf + bm + bs + bi);
             // one bulk copy per 16-byte chunk plane of the tile's cell range
 #pragma unroll
@@ -369,13 +393,13 @@ struct FaceIn {
     unsigned iter = 0;                                                                           \
     for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {                             \
         const int buf = iter & 1;                                                                \
-        unsigned char* st = smem + 128 + buf * L.stage;                                          \
+        unsigned char* st = smem + kHeader + buf * L.stage;                                      \
         mbar_wait(full + buf, (iter >> 1) & 1, a.err);                                           \
-        int base, nb, f0t, nft, h0t, nht, inst;                                                  \
-        tile_info<ARENA>(a, t, base, nb, f0t, nft, h0t, nht, inst);                              \
+        const StageInfo& si = reinterpret_cast<const StageInfo*>(smem + 64)[buf];                \
+        const int base = si.base, nb = si.nb, h0t = si.h0, inst = si.inst;                      \
         const Cell4<T>* sU = reinterpret_cast<const Cell4<T>*>(st + L.u);                        \
         const T* sGeo = reinterpret_cast<const T*>(st + L.geo);                                  \
-        const int nfl = reinterpret_cast<const int*>(smem + 64)[buf];                            \
+        const int nfl = si.nf;                                                                   \
         const short* sMeta = reinterpret_cast<const short*>(st + L.meta);                        \
         const short* sSlot = reinterpret_cast<const short*>(st + L.cslot);                       \
         const T* sIv = reinterpret_cast<const T*>(st + L.iv);
@@ -393,7 +417,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
     const StepArgs<T>& s = a.s;
     double dtc = 1e300;
     HCFD_TILE_LOOP_BEGIN(false, ARENA)
-    const int lmode = limiter_mode(ARENA ? a.inst_stats[inst].steps : s.stats->steps, s.freeze_after);
+    const int lmode = limiter_mode(si.steps, s.freeze_after);
     for (int c = threadIdx.x; c < nb; c += NT) {
         short cs[8];
         lds_slots(sSlot + c * a.Wp, a.Wp, cs);
@@ -505,19 +529,14 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const TileSmem<T> L(a.B, a.Hmax, a.Fmax, W, a.Wp, true);
     const StepArgs<T>& s = a.s;
-    double dt_used = (s.time_mode == TM_FIXED) ? s.dt_or_cfl
-                                                : s.dt_or_cfl * __longlong_as_double((long long) *s.dtmin);
+    double dt_used = 0.0;
     double r2 = 0.0;
     int bad = 0;
     __shared__ double s_wr2[8];
     __shared__ int s_wbad[8];
     HCFD_TILE_LOOP_BEGIN(true, ARENA)
-    T cfl_or_dt = T(s.dt_or_cfl);
-    if constexpr (ARENA) {
-        const double v = __ldg(a.inst_dt + inst);
-        cfl_or_dt = T(v);
-        dt_used = (s.time_mode == TM_FIXED) ? v : v * __longlong_as_double((long long) a.inst_dtmin[2 * inst + a.par]);
-    }
+    const T cfl_or_dt = T(si.dt_or_cfl);
+    dt_used = (s.time_mode == TM_FIXED) ? si.dt_or_cfl : si.dt_or_cfl * si.dtmin;
     const Grad8<T>* sG = reinterpret_cast<const Grad8<T>*>(st + L.g);
     const int nf = nfl;
     // face phase: one Rusanov flux per face entry (Flux.cpp:19-38).  Each thread takes two

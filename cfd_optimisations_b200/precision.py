@@ -9,10 +9,12 @@ Defaults are the 1025 x 513-node wedge (1,048,576 triangles), M 3.0, ramp 20 deg
 time stepping at CFL 0.8, Venkatakrishnan limiter K = 5, stop when the L2 density residual
 has dropped `orders` orders below its first value or after `max-steps`.  Without limiter
 freezing (--freeze N: steps after N reuse step N's limiter values) the residual of either
-limiter stalls after one or two orders, the limiter switching back and forth.  Prints one JSON object: for each precision the
-steps and device time to convergence, and the FP32 errors against FP64 — relative L-inf and
-L2 of each conserved variable, and the L-inf and L2 error of the wall pressure coefficient
-on the lower wall (the ramp).
+limiter stalls after one or two orders, the limiter switching back and forth.  Prints one
+JSON object: for each precision the steps and device time to convergence, and the FP32 errors
+against FP64 (relative L-inf and L2 of each conserved variable, and the L-inf and L2 error of
+the wall pressure coefficient on the lower wall, the ramp).  A third run, FP64 from an initial
+density one rounding step larger, gives the same errors for a perturbation the size of one
+rounding: the floor that no precision can go below while the limiter keeps switching.
 """
 from __future__ import annotations
 
@@ -31,12 +33,15 @@ LOWER_WALL = 2   # colour of the lower wall (the ramp) in the generated wedge
 
 def converge(mesh: Mesh, precision: int, mach: float, cfl: float, orders: float, max_steps: int,
              mode: int = LOCAL_CFL, limiter: int = LIMITER_VENKAT, K: float = 5.0, chunk: int = 200,
-             freeze: int = 0) -> dict:
-    """Runs one solve to convergence; returns its state, wall Cp and timing."""
+             freeze: int = 0, rho_scale: float = 1.0) -> dict:
+    """Runs one solve to convergence; returns its state, wall Cp and timing.  `rho_scale`
+    scales the initial density (1 + 2**-52: a perturbation the size of one rounding)."""
     bcmap, qbc, q = wedge_case(mach)
     s = Solver(mesh, limiter=limiter, venkat_K=K, precision=precision, freeze_limiter_after=freeze)
     s.gather_bcs(bcmap, qbc)
-    s.initialise(q)
+    qi = list(q)
+    qi[0] *= rho_scale
+    s.initialise(qi)
     steps, ms, hist = 0, 0.0, []
     st = s.step(1, mode, cfl)
     steps += 1
@@ -87,15 +92,19 @@ def study(nx=1025, ny=513, mach=3.0, theta=20.0, cfl=0.8, orders=8.0, max_steps=
                              max_steps=max_steps, limiter="venkatakrishnan" if limiter == LIMITER_VENKAT else "bj",
                              K=K, freeze_limiter_after=freeze))
     runs = {}
-    for name, prec in (("fp64", FP64), ("fp32", FP32)):
+    for name, prec, scale in (("fp64", FP64, 1.0), ("fp32", FP32, 1.0), ("fp64_perturbed", FP64, 1.0 + 2.0 ** -52)):
         t0 = time.perf_counter()
         runs[name] = converge(mesh, prec, mach, cfl, orders, max_steps, mode=mode, limiter=limiter, K=K,
-                              freeze=freeze)
+                              freeze=freeze, rho_scale=scale)
         r = runs[name]
         out[name] = dict(steps=r["steps"], device_ms=r["ms"], wall_s=time.perf_counter() - t0, diverged=r["diverged"],
                          residual_drop_orders=r["drop"], converged=bool(r["drop"] is not None and r["drop"] >= orders))
-    out["fp32_vs_fp64"] = (errors(runs["fp32"], runs["fp64"]) if runs["fp32"]["U"] is not None and
-                           runs["fp64"]["U"] is not None else None)
+    ok = lambda k: runs[k]["U"] is not None
+    out["fp32_vs_fp64"] = errors(runs["fp32"], runs["fp64"]) if ok("fp32") and ok("fp64") else None
+    # the same FP64 solve from an initial density one rounding step larger: the spread that
+    # rounding alone gives in this solve, whatever the precision
+    out["fp64_perturbed_vs_fp64"] = (errors(runs["fp64_perturbed"], runs["fp64"])
+                                     if ok("fp64_perturbed") and ok("fp64") else None)
     return out
 
 

@@ -38,7 +38,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import FP32, FP64, GLOBAL_CFL, KERNEL_CELL, LIMITER_BJ, NUMBER_RANDOM, Mesh, Solver, wedge_case
+from . import FP32, FP64, GLOBAL_CFL, LIMITER_BJ, NUMBER_RANDOM, Mesh, Solver, wedge_case
+from .native import ENONFINITE, HcfdError
 
 
 @dataclass
@@ -193,17 +194,26 @@ class Server:
         return sorted(results, key=lambda x: x.rid)
 
 
-def solve_alone_fp64(r: Request, cfl: float, orders: float, max_steps: int, chunk: int, **kw):
-    """One request through the plain FP64 solver; returns (device ms, Result-like dict, U)."""
+def solve_alone_fp64(r: Request, cfl: float, orders: float, max_steps: int, chunk: int, rho_scale: float = 1.0,
+                     **kw):
+    """One request through the plain FP64 solver; returns (device ms, Result-like dict, U).
+    `rho_scale` scales the initial density (a rounding-sized perturbation with 1 + 2**-52)."""
     bcmap, qbc, q = wedge_case(r.mach)
     s = Solver(build_mesh(r), precision=FP64, limiter=LIMITER_BJ, **kw)
     s.gather_bcs(bcmap, qbc)
-    s.initialise(q)
+    qi = list(q)
+    qi[0] *= rho_scale
+    s.initialise(qi)
     ms, steps = 0.0, 0
     while True:
-        ms += s.step_timed(chunk, GLOBAL_CFL, cfl)
+        try:
+            ms += s.step_timed(chunk, GLOBAL_CFL, cfl)
+            st = s.stats()
+        except HcfdError as e:
+            if e.code != ENONFINITE:
+                raise
+            st = dict(res_l2=0.0, res_first=0.0, nonfinite=True)
         steps += chunk
-        st = s.stats()
         st["steps"] = steps
         why = done_reason(st, orders, max_steps)
         if why is not None:
@@ -273,9 +283,9 @@ def main():
         den = np.abs(U64).max(axis=1)
         errs.append(dict(rid=r.rid, triangles=r.triangles, steps_fp32=served.steps, steps_fp64=info["steps"],
                          rel_linf=float((np.abs(served.U - U64).max(axis=1) / den).max())))
-        # the same FP64 solve by the per-cell kernels: it differs from the tiled one only in
-        # the rounding of fused multiply-adds, so this is the spread that rounding alone gives
-        _, info2, U64b = solve_alone_fp64(r, a.cfl, a.orders, a.max_steps, a.chunk, kernel=KERNEL_CELL)
+        # the same FP64 solve from an initial density one rounding step larger: the spread
+        # that rounding alone produces in this solve, whatever the precision
+        _, info2, U64b = solve_alone_fp64(r, a.cfl, a.orders, a.max_steps, a.chunk, rho_scale=1.0 + 2.0 ** -52)
         errs64.append(float((np.abs(U64b - U64).max(axis=1) / den).max()))
     per_cell_step = sum(s for _, s, _ in base) / sum(r.triangles * i["steps"] for r, _, i in base)
     # sequential service of the whole stream, each request's time estimated from its cell-steps
@@ -293,7 +303,8 @@ def main():
     out["speedup_solves_per_s"] = out["served"]["solves_per_s"] / out["fp64_sequential"]["solves_per_s"]
     e32 = [e["rel_linf"] for e in errs]
     out["fp32_vs_fp64_rel_linf"] = dict(n=len(e32), max=max(e32), median=float(np.median(e32)), per_request=errs)
-    out["fp64_tiled_vs_fp64_cell_rel_linf"] = dict(n=len(errs64), max=max(errs64), median=float(np.median(errs64)))
+    out["fp64_vs_fp64_initial_density_plus_one_ulp_rel_linf"] = dict(n=len(errs64), max=max(errs64),
+                                                                    median=float(np.median(errs64)))
     print(json.dumps(out))
 
 
