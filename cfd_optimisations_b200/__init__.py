@@ -18,6 +18,7 @@ solver call raises.
 from __future__ import annotations
 
 import ctypes as ct
+import os
 
 import numpy as np
 
@@ -199,20 +200,67 @@ class Solver:
         ptrs = (ct.POINTER(ct.c_double) * 4)(*[_dptr(U[v]) for v in range(4)])
         _n.check(_n.lib().hcfd_gpu_upload(self._h, ptrs))
 
+    def snapshot(self, out: np.ndarray, prims: bool = True) -> "Snapshot":
+        """Starts copying the current state into `out` (4 x Nc float64, C order; pin it with
+        `pin` for the copy to overlap later steps) and returns at once."""
+        if out.shape != (4, self.Nc) or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("snapshot: out must be a C-contiguous float64 array of shape (4, Nc)")
+        ptrs = (_n._dp * 4)(*[out[v].ctypes.data_as(_n._dp) for v in range(4)])
+        t = ct.c_void_p()
+        _n.check(_n.lib().hcfd_gpu_snapshot(self._h, 1 if prims else 0, ptrs, ct.byref(t)))
+        return Snapshot(t, out)
+
+    def checkpoint(self, path: str) -> None:
+        """Exact snapshot (state, step statistics, recorded limiter values) for resuming."""
+        _n.check(_n.lib().hcfd_gpu_checkpoint(self._h, os.fsencode(path)))
+
+    def restore(self, path: str) -> None:
+        """Continues a checkpointed solve: the next steps are bit-identical to the original's."""
+        _n.check(_n.lib().hcfd_gpu_restore(self._h, os.fsencode(path)))
+
     def wall_cp(self, colour: int, rho_inf: float, p_inf: float, speed_inf: float) -> np.ndarray:
         out = np.empty(self.Nf)
         n = ct.c_int()
         _n.check(_n.lib().hcfd_gpu_wall_cp(self._h, colour, rho_inf, p_inf, speed_inf, _dptr(out), ct.byref(n)))
         return out[:n.value].copy()
 
-    def profile(self, enable: bool) -> None:
-        _n.check(_n.lib().hcfd_gpu_profile(self._h, 1 if enable else 0))
+    def profile(self, enable, every: int = 1) -> None:
+        """Per-kernel CUDA-event timing of every `every`-th step while enabled."""
+        _n.check(_n.lib().hcfd_gpu_profile(self._h, max(1, int(every)) if enable else 0))
 
     def profile_read(self) -> dict:
         m1, m2 = ct.c_double(), ct.c_double()
         n1, n2 = ct.c_longlong(), ct.c_longlong()
         _n.check(_n.lib().hcfd_gpu_profile_read(self._h, ct.byref(m1), ct.byref(n1), ct.byref(m2), ct.byref(n2)))
         return dict(ms_pass1=m1.value, n_pass1=n1.value, ms_pass2=m2.value, n_pass2=n2.value)
+
+
+class Snapshot:
+    """A snapshot in flight (Solver.snapshot): wait() returns the filled array."""
+
+    def __init__(self, h, out: np.ndarray):
+        self._h = h
+        self.out = out
+
+    def wait(self) -> np.ndarray:
+        if self._h is not None:
+            _n.check(_n.lib().hcfd_snapshot_wait(self._h))
+        return self.out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _n.lib().hcfd_snapshot_free(h)
+            self._h = None
+
+
+def checkpoint_info(path: str) -> dict:
+    """Header of a checkpoint file (no GPU needed)."""
+    nc, prec, hl = ct.c_int(), ct.c_int(), ct.c_int()
+    steps = ct.c_longlong()
+    _n.check(_n.lib().hcfd_checkpoint_info(os.fsencode(path), ct.byref(nc), ct.byref(prec), ct.byref(steps),
+                                           ct.byref(hl)))
+    return dict(Nc=nc.value, precision=prec.value, steps=steps.value, has_limiter=bool(hl.value))
 
 
 def plan_check(mesh: Mesh, tile: int = 0, keep_numbering: bool = False) -> dict:

@@ -75,7 +75,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
         subprocess.run(cmd, check=True)
     drv_src = os.path.join(CSRC, "drivers", "wedge_driver.cpp")
     if os.path.exists(drv_src) and (force or _stale(DRIVER, [drv_src, LIB] + _deps())):
-        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, drv_src, "-o", DRIVER,
+        cmd = ["g++", "-O2", "-std=c++17", "-pthread", "-I", INCLUDE, drv_src, "-o", DRIVER,
                "-L", LIBDIR, "-lhcfd_gpu", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)

@@ -3,6 +3,7 @@ building block of the serving loop (serve.py)."""
 from __future__ import annotations
 
 import ctypes as ct
+import os
 
 import numpy as np
 
@@ -90,6 +91,14 @@ class Arena:
         ptrs = (ct.POINTER(ct.c_double) * 4)(*[out[v].ctypes.data_as(_n._dp) for v in range(4)])
         _n.check(_n.lib().hcfd_arena_fetch(self._h, slot, 1 if prims else 0, ptrs))
         return out
+
+    def checkpoint(self, slot: int, path: str) -> None:
+        """Exact snapshot of one instance (the format of Solver.checkpoint)."""
+        _n.check(_n.lib().hcfd_arena_checkpoint(self._h, slot, os.fsencode(path)))
+
+    def restore(self, slot: int, path: str) -> None:
+        """Loads a checkpoint into an admitted instance of the same mesh."""
+        _n.check(_n.lib().hcfd_arena_restore(self._h, slot, os.fsencode(path)))
 
     def release(self, slot: int) -> None:
         _n.check(_n.lib().hcfd_arena_release(self._h, slot))

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <string>
@@ -157,6 +158,17 @@ template <class T>
 __global__ void arena_iv_kernel(int n, const double* __restrict__ ivu, const int* __restrict__ perm, T* __restrict__ iv) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) iv[i] = T(ivu[perm[i]]);
+}
+
+// Instance cells (internal order, from arena cell c0) from 4 x n doubles in input numbering.
+template <class T>
+__global__ void arena_in_kernel(size_t ps, size_t c0, int n, const double* __restrict__ in, const int* __restrict__ perm,
+                                Cell4<T>* U) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t j = perm[i];
+    const T u[4] = {T(in[j]), T(in[(size_t) n + j]), T(in[2 * (size_t) n + j]), T(in[3 * (size_t) n + j])};
+    hcfd::st_cell(U, ps, (int) (c0 + i), u);
 }
 
 // dst[k] = c0 + map[src[k]]: input cell numbers -> arena cell numbers.
@@ -739,6 +751,90 @@ int hcfd_arena_fetch(hcfd_arena* A, int slot, int prims, double* const* out) {
     cudaFreeAsync(d_out, A->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
     if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("arena_fetch: ") + cudaGetErrorString(e));
+    return HCFD_OK;
+}
+
+// One instance's exact snapshot, in the file format of hcfd_gpu_checkpoint.
+int hcfd_arena_checkpoint(hcfd_arena* A, int slot, const char* path) {
+    hcfd::clear_error();
+    if (!A || slot < 0 || slot >= (int) A->inst.size() || !A->inst[slot].active || !path)
+        return fail(HCFD_EINVAL, "arena_checkpoint: bad argument");
+    CK(cudaSetDevice(A->device));
+    const Inst& I = A->inst[slot];
+    const size_t n = 4 * (size_t) I.Nc;
+    const bool frz = A->phiF != nullptr;
+    std::vector<double> U(n), phi(frz ? n : 0);
+    hcfd::StepStats st{};
+    double* d_out = nullptr;
+    CK(cudaMallocAsync((void**) &d_out, sizeof(double) * n, A->stream));
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < (frz ? 2 : 1) && e == cudaSuccess; k++) {
+        const void* src = k == 0 ? A->U[A->cur] : A->phiF;
+        if (A->fp32())
+            arena_out_kernel<float><<<nblk(I.Nc, 256), 256, 0, A->stream>>>(A->Ccap, I.c0, I.Nc, (const Cell4<float>*) src, I.d_perm, A->prm.gma, 0, d_out);
+        else
+            arena_out_kernel<double><<<nblk(I.Nc, 256), 256, 0, A->stream>>>(A->Ccap, I.c0, I.Nc, (const Cell4<double>*) src, I.d_perm, A->prm.gma, 0, d_out);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(k == 0 ? U.data() : phi.data(), d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, A->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&st, A->stats + slot, sizeof(st), cudaMemcpyDeviceToHost, A->stream);
+    cudaFreeAsync(d_out, A->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+    if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("arena_checkpoint: ") + cudaGetErrorString(e));
+    hcfd::CkptHeader h{};
+    std::memcpy(h.magic, "HCFDCKP1", 8);
+    h.version = 1;
+    h.precision = A->prm.precision;
+    h.Nc = I.Nc;
+    h.has_phiF = frz ? 1 : 0;
+    h.steps = st.steps;
+    h.res2_first = st.res2_first;
+    h.res2_last = st.res2_last;
+    h.dt_last = st.dt_last;
+    h.nonfinite = st.nonfinite;
+    return hcfd::ckpt_write(path, h, U, frz ? &phi : nullptr);
+}
+
+// Restores a checkpoint into an admitted instance of the same mesh (its state, statistics
+// and recorded limiter values): its next steps continue the original solve bit for bit.
+int hcfd_arena_restore(hcfd_arena* A, int slot, const char* path) {
+    hcfd::clear_error();
+    if (!A || slot < 0 || slot >= (int) A->inst.size() || !A->inst[slot].active || !path)
+        return fail(HCFD_EINVAL, "arena_restore: bad argument");
+    CK(cudaSetDevice(A->device));
+    const Inst& I = A->inst[slot];
+    hcfd::CkptHeader h;
+    std::vector<double> U, phi;
+    int rc = hcfd::ckpt_read(path, h, &U, &phi);
+    if (rc) return rc;
+    const bool frz = A->phiF != nullptr;
+    if (h.Nc != I.Nc) return fail(HCFD_EINVAL, "arena_restore: the checkpoint is of a mesh with another cell count");
+    if (h.precision != A->prm.precision) return fail(HCFD_EINVAL, "arena_restore: the checkpoint is of another precision");
+    if ((h.has_phiF != 0) != frz) return fail(HCFD_EINVAL, "arena_restore: limiter freezing differs");
+    const size_t n = 4 * (size_t) I.Nc;
+    double* d_in = nullptr;
+    CK(cudaMallocAsync((void**) &d_in, sizeof(double) * n, A->stream));
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < (frz ? 2 : 1) && e == cudaSuccess; k++) {
+        void* dst = k == 0 ? A->U[A->cur] : A->phiF;
+        e = cudaMemcpyAsync(d_in, k == 0 ? U.data() : phi.data(), sizeof(double) * n, cudaMemcpyHostToDevice, A->stream);
+        if (e != cudaSuccess) break;
+        if (A->fp32()) arena_in_kernel<float><<<nblk(I.Nc, 256), 256, 0, A->stream>>>(A->Ccap, I.c0, I.Nc, d_in, I.d_perm, (Cell4<float>*) dst);
+        else arena_in_kernel<double><<<nblk(I.Nc, 256), 256, 0, A->stream>>>(A->Ccap, I.c0, I.Nc, d_in, I.d_perm, (Cell4<double>*) dst);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+    }
+    hcfd::StepStats st{};
+    st.res2_first = h.res2_first;
+    st.res2_last = h.res2_last;
+    st.dt_last = h.dt_last;
+    st.steps = h.steps;
+    st.nonfinite = h.nonfinite;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(A->stats + slot, &st, sizeof(st), cudaMemcpyHostToDevice, A->stream);
+    cudaFreeAsync(d_in, A->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(A->stream);
+    if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("arena_restore: ") + cudaGetErrorString(e));
     return HCFD_OK;
 }
 

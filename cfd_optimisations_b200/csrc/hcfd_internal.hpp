@@ -46,3 +46,23 @@ int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, con
                     const std::vector<char>& ghost, const std::vector<int>& perm, int F_BC,
                     const std::vector<int>& bc_first, int B, int W, TilePlan& P);
 }  // namespace hcfd
+
+namespace hcfd {
+// Checkpoint file of one solve (hcfd_gpu_checkpoint / hcfd_arena_checkpoint): this header,
+// then the conservative state of every cell, variable-major, in the input numbering, as
+// doubles (FP32 values widen exactly), then, with limiter freezing, the recorded limiter
+// values in the same layout.
+struct CkptHeader {
+    char magic[8];               // "HCFDCKP1"
+    int version;                 // 1
+    int precision;               // enum hcfd_precision of the solve
+    int Nc;
+    int has_phiF;
+    long long steps;
+    double res2_first, res2_last, dt_last;
+    int nonfinite, pad;
+};
+int ckpt_write(const char* path, const CkptHeader& h, const std::vector<double>& U, const std::vector<double>* phiF);
+int ckpt_read(const char* path, CkptHeader& h, std::vector<double>* U, std::vector<double>* phiF);
+}  // namespace hcfd
+

@@ -579,6 +579,68 @@ int hcfd_write_hsln(const char* path, int nvars, const char* const* varnames, in
     return ok ? HCFD_OK : fail(HCFD_EIO, "write_hsln: write failed");
 }
 
+int hcfd_checkpoint_info(const char* path, int* Nc, int* precision, long long* steps, int* has_limiter) {
+    hcfd::clear_error();
+    if (!path) return fail(HCFD_EINVAL, "checkpoint_info: null path");
+    hcfd::CkptHeader h;
+    int rc = hcfd::ckpt_read(path, h, nullptr, nullptr);
+    if (rc) return rc;
+    if (Nc) *Nc = h.Nc;
+    if (precision) *precision = h.precision;
+    if (steps) *steps = h.steps;
+    if (has_limiter) *has_limiter = h.has_phiF;
+    return HCFD_OK;
+}
+
 const char* hcfd_last_error(void) { return hcfd::g_err.c_str(); }
 
 }  // extern "C"
+
+namespace hcfd {
+
+int ckpt_write(const char* path, const CkptHeader& h, const std::vector<double>& U, const std::vector<double>* phiF) {
+    if (!path) return fail(HCFD_EINVAL, "checkpoint: null path");
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return fail(HCFD_EIO, std::string("checkpoint: cannot open ") + path);
+    bool ok = fwrite(&h, sizeof(h), 1, fp) == 1 && fwrite(U.data(), 8, U.size(), fp) == U.size();
+    if (ok && phiF) ok = fwrite(phiF->data(), 8, phiF->size(), fp) == phiF->size();
+    ok = (fclose(fp) == 0) && ok;
+    return ok ? HCFD_OK : fail(HCFD_EIO, std::string("checkpoint: write failed: ") + path);
+}
+
+int ckpt_read(const char* path, CkptHeader& h, std::vector<double>* U, std::vector<double>* phiF) {
+    FILE* fp = fopen(path, "rb");
+    if (!fp) return fail(HCFD_EIO, std::string("checkpoint: cannot open ") + path);
+    auto bad = [&](const char* why) {
+        fclose(fp);
+        return fail(HCFD_EIO, std::string("checkpoint: ") + why + ": " + path);
+    };
+    if (fread(&h, sizeof(h), 1, fp) != 1) return bad("short header");
+    if (std::memcmp(h.magic, "HCFDCKP1", 8) != 0 || h.version != 1) return bad("not a checkpoint of this library");
+    if (h.Nc <= 0 || (h.precision != HCFD_FP64 && h.precision != HCFD_FP32) || (h.has_phiF != 0 && h.has_phiF != 1) ||
+        h.steps < 0)
+        return bad("corrupt header");
+    const size_t n = 4 * (size_t) h.Nc;
+    if (U) {
+        U->resize(n);
+        if (fread(U->data(), 8, n, fp) != n) return bad("short state");
+    } else if (fseek(fp, (long) (8 * n), SEEK_CUR) != 0) {
+        return bad("short state");
+    }
+    if (h.has_phiF) {
+        if (phiF) {
+            phiF->resize(n);
+            if (fread(phiF->data(), 8, n, fp) != n) return bad("short limiter values");
+        }
+    }
+    // nothing may follow the declared data
+    if (U && (!h.has_phiF || phiF)) {
+        char c;
+        if (fread(&c, 1, 1, fp) == 1) return bad("trailing bytes");
+    }
+    fclose(fp);
+    return HCFD_OK;
+}
+
+}  // namespace hcfd
+

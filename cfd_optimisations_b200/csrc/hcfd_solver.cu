@@ -101,7 +101,15 @@ struct hcfd_solver {
     int block = 256;
     int partial_len = 0;
     // profiling
+    // asynchronous snapshots (hcfd_gpu_snapshot): staging buffer, copy stream, and the event
+    // after which the staging buffer may be overwritten
+    double* d_snap = nullptr;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t snap_free = nullptr;
+    bool snap_used = false;
     bool prof = false;
+    int prof_every = 1;                  // record every prof_every-th step
+    long long prof_count = 0;
     std::vector<cudaEvent_t> ev1, ev2;   // start/stop pairs per launch
     double ms1 = 0, ms2 = 0;
     long long n1 = 0, n2 = 0;
@@ -124,6 +132,10 @@ void free_all(hcfd_solver* s) {
         void* q[] = {P.d_tgeo, P.d_tmeta, P.d_foff, P.d_hoff, P.d_halo, P.d_cslot, P.d_efid};
         for (void* p : q) if (p) cudaFree(p);
     }
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+    if (s->d_snap) cudaFree(s->d_snap);
+    if (s->snap_free) cudaEventDestroy(s->snap_free);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -185,15 +197,15 @@ struct Ev {
     cudaEvent_t a = nullptr, b = nullptr;
 };
 
-int prof_begin(hcfd_solver* s, Ev& e) {
-    if (!s->prof) return HCFD_OK;
+int prof_begin(hcfd_solver* s, bool rec, Ev& e) {
+    if (!rec) return HCFD_OK;
     CK(cudaEventCreate(&e.a));
     CK(cudaEventCreate(&e.b));
     CK(cudaEventRecord(e.a, s->stream));
     return HCFD_OK;
 }
-int prof_end(hcfd_solver* s, Ev& e, std::vector<cudaEvent_t>& into) {
-    if (!s->prof) return HCFD_OK;
+int prof_end(hcfd_solver* s, bool rec, Ev& e, std::vector<cudaEvent_t>& into) {
+    if (!rec) return HCFD_OK;
     CK(cudaEventRecord(e.b, s->stream));
     into.push_back(e.a);
     into.push_back(e.b);
@@ -204,25 +216,26 @@ template <class T, int W>
 int launch_step(hcfd_solver* s, int time_mode, double dt_or_cfl) {
     Ev e1, e2;
     int rc;
+    const bool rec = s->prof && (s->prof_count++ % s->prof_every == 0);
     if (s->tiled) {
         const TiledPass& P2 = s->split ? s->tp[1] : s->tp[0];
         const hcfd::TileArgs<T> a1 = tile_args<T>(s, time_mode, dt_or_cfl, s->tp[0]);
         const hcfd::TileArgs<T> a2 = tile_args<T>(s, time_mode, dt_or_cfl, P2);
-        if ((rc = prof_begin(s, e1))) return rc;
+        if ((rc = prof_begin(s, rec, e1))) return rc;
         hcfd::tile_pass1_kernel<T, W, false><<<s->grid1, s->tp[0].block + 32, s->smem1, s->stream>>>(a1);
-        if ((rc = prof_end(s, e1, s->ev1))) return rc;
-        if ((rc = prof_begin(s, e2))) return rc;
+        if ((rc = prof_end(s, rec, e1, s->ev1))) return rc;
+        if ((rc = prof_begin(s, rec, e2))) return rc;
         hcfd::tile_pass2_kernel<T, W, std::is_same<T, float>::value, false><<<s->grid2, P2.block + 32, s->smem2, s->stream>>>(a2);
-        if ((rc = prof_end(s, e2, s->ev2))) return rc;
+        if ((rc = prof_end(s, rec, e2, s->ev2))) return rc;
     } else {
         const int grid = nblk(s->Nc, s->block);
         hcfd::StepArgs<T> a = step_args<T>(s, time_mode, dt_or_cfl);
-        if ((rc = prof_begin(s, e1))) return rc;
+        if ((rc = prof_begin(s, rec, e1))) return rc;
         hcfd::pass1_kernel<T, W><<<grid, s->block, 0, s->stream>>>(a);
-        if ((rc = prof_end(s, e1, s->ev1))) return rc;
-        if ((rc = prof_begin(s, e2))) return rc;
+        if ((rc = prof_end(s, rec, e1, s->ev1))) return rc;
+        if ((rc = prof_begin(s, rec, e2))) return rc;
         hcfd::pass2_kernel<T, W, std::is_same<T, float>::value><<<grid, s->block, 0, s->stream>>>(a);
-        if ((rc = prof_end(s, e2, s->ev2))) return rc;
+        if ((rc = prof_end(s, rec, e2, s->ev2))) return rc;
     }
     CK(cudaGetLastError());
     s->cur = 1 - s->cur;
@@ -658,6 +671,149 @@ int hcfd_gpu_upload(hcfd_solver* s, const double* const* in) {
     return HCFD_OK;
 }
 
+}  // extern "C"
+
+// A snapshot in flight: done when its copies to the host have landed.
+struct hcfd_snapshot {
+    cudaEvent_t done = nullptr;
+    int device = 0;
+};
+
+extern "C" {
+
+int hcfd_gpu_snapshot(hcfd_solver* s, int prims, double* const* host, hcfd_snapshot** ticket) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!host || !ticket) return fail(HCFD_EINVAL, "snapshot: null argument");
+    for (int v = 0; v < 4; v++) if (!host[v]) return fail(HCFD_EINVAL, "snapshot: null host array");
+    *ticket = nullptr;
+    if (!s->d_snap) {
+        // first snapshot: staging buffer, copy stream and event (allocates once)
+        CK(cudaMalloc((void**) &s->d_snap, sizeof(double) * 4 * (size_t) s->Nc));
+        CK(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&s->snap_free, cudaEventDisableTiming));
+    }
+    auto t = std::make_unique<hcfd_snapshot>();
+    t->device = s->device;
+    CK(cudaEventCreateWithFlags(&t->done, cudaEventDisableTiming));
+    auto bail = [&](int code) { cudaEventDestroy(t->done); return code; };
+    cudaError_t e = cudaSuccess;
+    // the staging buffer is free once the previous snapshot's copies have landed
+    if (s->snap_used) e = cudaStreamWaitEvent(s->stream, s->snap_free, 0);
+    if (e == cudaSuccess) {
+        if (s->fp32()) hcfd::out_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<float>*) s->d_U[s->cur], s->d_perm, s->prm.gma, prims, s->d_snap);
+        else hcfd::out_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<double>*) s->d_U[s->cur], s->d_perm, s->prm.gma, prims, s->d_snap);
+        e = cudaGetLastError();
+    }
+    // the copy stream starts when the conversion is done; the solver stream goes on stepping
+    cudaEvent_t ready = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ready, s->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy_stream, ready, 0);
+    if (ready) cudaEventDestroy(ready);
+    for (int v = 0; v < 4 && e == cudaSuccess; v++)
+        e = cudaMemcpyAsync(host[v], s->d_snap + (size_t) v * s->Nc, sizeof(double) * s->Nc, cudaMemcpyDeviceToHost,
+                            s->copy_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(s->snap_free, s->copy_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(t->done, s->copy_stream);
+    if (e != cudaSuccess) return bail(fail(HCFD_ECUDA, std::string("snapshot: ") + cudaGetErrorString(e)));
+    s->snap_used = true;
+    *ticket = t.release();
+    return HCFD_OK;
+}
+
+int hcfd_snapshot_wait(hcfd_snapshot* t) {
+    hcfd::clear_error();
+    if (!t) return fail(HCFD_EINVAL, "snapshot_wait: null ticket");
+    const cudaError_t e = cudaEventSynchronize(t->done);
+    if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("snapshot_wait: ") + cudaGetErrorString(e));
+    return HCFD_OK;
+}
+
+void hcfd_snapshot_free(hcfd_snapshot* t) {
+    if (!t) return;
+    if (t->done) {
+        cudaEventSynchronize(t->done);
+        cudaEventDestroy(t->done);
+    }
+    delete t;
+}
+
+// Exact snapshot of a solve: the conservative state (all cells, input numbering), the step
+// statistics and, with limiter freezing, the recorded limiter values.
+int hcfd_gpu_checkpoint(hcfd_solver* s, const char* path) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!path) return fail(HCFD_EINVAL, "checkpoint: null path");
+    if (!s->initialised) return fail(HCFD_EINVAL, "checkpoint: solver not initialised");
+    const size_t n = 4 * (size_t) s->Nc;
+    std::vector<double> U(n), phi;
+    hcfd::StepStats st{};
+    auto grab = [&](const void* src, std::vector<double>& dst) -> int {
+        if (s->fp32()) hcfd::out_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<float>*) src, s->d_perm, s->prm.gma, 0, s->d_io);
+        else hcfd::out_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, (const hcfd::Cell4<double>*) src, s->d_perm, s->prm.gma, 0, s->d_io);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(dst.data(), s->d_io, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        return HCFD_OK;
+    };
+    if ((rc = grab(s->d_U[s->cur], U))) return rc;
+    if (s->d_phiF) {
+        phi.resize(n);
+        if ((rc = grab(s->d_phiF, phi))) return rc;
+    }
+    CK(cudaMemcpyAsync(&st, s->d_stats, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    hcfd::CkptHeader h{};
+    std::memcpy(h.magic, "HCFDCKP1", 8);
+    h.version = 1;
+    h.precision = s->prm.precision;
+    h.Nc = s->Nc;
+    h.has_phiF = s->d_phiF ? 1 : 0;
+    h.steps = st.steps;
+    h.res2_first = st.res2_first;
+    h.res2_last = st.res2_last;
+    h.dt_last = st.dt_last;
+    h.nonfinite = st.nonfinite;
+    return hcfd::ckpt_write(path, h, U, s->d_phiF ? &phi : nullptr);
+}
+
+int hcfd_gpu_restore(hcfd_solver* s, const char* path) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!path) return fail(HCFD_EINVAL, "restore: null path");
+    hcfd::CkptHeader h;
+    std::vector<double> U, phi;
+    if ((rc = hcfd::ckpt_read(path, h, &U, &phi))) return rc;
+    if (h.Nc != s->Nc) return fail(HCFD_EINVAL, "restore: the checkpoint is of a mesh with another cell count");
+    if (h.precision != s->prm.precision) return fail(HCFD_EINVAL, "restore: the checkpoint is of another precision");
+    if ((h.has_phiF != 0) != (s->d_phiF != nullptr))
+        return fail(HCFD_EINVAL, "restore: limiter freezing differs between the checkpoint and this solver");
+    auto put = [&](const std::vector<double>& src, void* dst) -> int {
+        CK(cudaMemcpyAsync(s->d_io, src.data(), sizeof(double) * src.size(), cudaMemcpyHostToDevice, s->stream));
+        if (s->fp32()) hcfd::in_kernel<float><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, s->d_io, s->d_perm, (hcfd::Cell4<float>*) dst);
+        else hcfd::in_kernel<double><<<nblk(s->Nc, 256), 256, 0, s->stream>>>(s->Nc, s->d_io, s->d_perm, (hcfd::Cell4<double>*) dst);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s->stream));   // d_io is reused by the next put
+        return HCFD_OK;
+    };
+    if ((rc = put(U, s->d_U[s->cur]))) return rc;
+    if (s->d_phiF && (rc = put(phi, s->d_phiF))) return rc;
+    hcfd::StepStats st{};
+    st.res2_first = h.res2_first;
+    st.res2_last = h.res2_last;
+    st.dt_last = h.dt_last;
+    st.steps = h.steps;
+    st.nonfinite = h.nonfinite;
+    CK(cudaMemcpyAsync(s->d_stats, &st, sizeof(st), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->initialised = true;
+    return HCFD_OK;
+}
+
 int hcfd_gpu_wall_cp(hcfd_solver* s, int colour, double rho_inf, double p_inf, double speed_inf, double* out, int* n) {
     hcfd::clear_error();
     int rc = check_handle(s);
@@ -692,7 +848,10 @@ int hcfd_gpu_profile(hcfd_solver* s, int enable) {
     for (auto e : s->ev2) cudaEventDestroy(e);
     s->ev1.clear(); s->ev2.clear();
     s->ms1 = s->ms2 = 0; s->n1 = s->n2 = 0;
+    if (enable < 0) return fail(HCFD_EINVAL, "profile: negative sampling period");
     s->prof = enable != 0;
+    s->prof_every = enable > 0 ? enable : 1;
+    s->prof_count = 0;
     return HCFD_OK;
 }
 

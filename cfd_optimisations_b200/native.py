@@ -109,6 +109,14 @@ _SIGS = {
     "hcfd_plan_check": (ct.c_int, [ct.POINTER(MeshView), ct.c_int, ct.c_int, ct.POINTER(ct.c_longlong)]),
     "hcfd_step_noalloc": (ct.c_int, [ct.POINTER(NoallocMesh), ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_double,
                                      ct.c_void_p, _dp, _dp]),
+    "hcfd_gpu_snapshot": (ct.c_int, [ct.c_void_p, ct.c_int, ct.POINTER(_dp), ct.POINTER(ct.c_void_p)]),
+    "hcfd_snapshot_wait": (ct.c_int, [ct.c_void_p]),
+    "hcfd_snapshot_free": (None, [ct.c_void_p]),
+    "hcfd_gpu_checkpoint": (ct.c_int, [ct.c_void_p, ct.c_char_p]),
+    "hcfd_gpu_restore": (ct.c_int, [ct.c_void_p, ct.c_char_p]),
+    "hcfd_checkpoint_info": (ct.c_int, [ct.c_char_p, _ip, _ip, ct.POINTER(ct.c_longlong), _ip]),
+    "hcfd_arena_checkpoint": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_char_p]),
+    "hcfd_arena_restore": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_char_p]),
     "hcfd_arena_create": (ct.c_int, [ct.POINTER(ArenaParams), ct.POINTER(ct.c_void_p)]),
     "hcfd_arena_admit": (ct.c_int, [ct.c_void_p, ct.POINTER(MeshView), _ip, ct.c_int, _dp, _dp, ct.c_double, _ip]),
     "hcfd_arena_prepare": (ct.c_int, [ct.c_void_p, ct.POINTER(MeshView), _ip, ct.c_int, _dp, _dp, ct.c_double,

@@ -185,6 +185,32 @@ int  hcfd_gpu_download(hcfd_solver* s, int prims, double* const* out);
 /* Overwrites the conservative state from 4 host arrays of Nc doubles (checkpoint
  * restore; no reference counterpart). */
 int  hcfd_gpu_upload(hcfd_solver* s, const double* const* in);
+/* Checkpoint and resume (no reference counterpart: the reference's only output is the .hsln
+ * snapshot of primitive variables, src/Euler.cpp:99-103, whose round trip to conservative
+ * variables is inexact, and it has no reader).  hcfd_gpu_checkpoint writes the conservative
+ * state of every cell (input numbering, doubles; FP32 values widen exactly), the step
+ * statistics and, with limiter freezing, the recorded limiter values.  hcfd_gpu_restore loads
+ * such a file into a solver made for the same mesh with the same parameters (BCs gathered):
+ * the following steps are bit-identical to the uninterrupted solve.  HCFD_EIO for a file
+ * that is not a checkpoint, HCFD_EINVAL for one of another mesh size, precision or freezing
+ * setting.  hcfd_checkpoint_info reads a checkpoint's header (no GPU needed). */
+/* Output without stopping the steps (no reference counterpart: Writer::write_soln,
+ * src/Writer.cpp:22-39, runs between steps while the loop waits).  hcfd_gpu_snapshot converts
+ * the current state (prims != 0: primitive) into a device staging buffer on the handle's
+ * stream and copies it into the 4 host arrays of Nc doubles on a second stream, then returns
+ * a ticket at once: later steps run while the copy is in flight.  Page-locked host arrays
+ * (hcfd_host_pin) are needed for the copy to overlap; with pageable ones the call returns
+ * only when the copy has landed.  hcfd_snapshot_wait blocks until the host arrays hold the
+ * snapshot; it touches only the ticket, so a writer thread may call it while another thread
+ * steps the solver.  hcfd_snapshot_free waits, then releases the ticket.  The first snapshot
+ * allocates the staging buffer, a stream and an event. */
+typedef struct hcfd_snapshot hcfd_snapshot;
+int  hcfd_gpu_snapshot(hcfd_solver* s, int prims, double* const* host, hcfd_snapshot** ticket);
+int  hcfd_snapshot_wait(hcfd_snapshot* t);
+void hcfd_snapshot_free(hcfd_snapshot* t);
+int  hcfd_gpu_checkpoint(hcfd_solver* s, const char* path);
+int  hcfd_gpu_restore(hcfd_solver* s, const char* path);
+int  hcfd_checkpoint_info(const char* path, int* Nc, int* precision, long long* steps, int* has_limiter);
 /* Waits for the handle's stream; returns HCFD_ENONFINITE if a step produced a NaN/Inf. */
 int  hcfd_gpu_sync(hcfd_solver* s);
 /* Statistics of the steps taken so far (waits for the stream). */
@@ -196,9 +222,10 @@ int  hcfd_gpu_wall_cp(hcfd_solver* s, int colour, double rho_inf, double p_inf, 
 /* Mesh facts as the solver sees them: Nc, Nf, number of real (non-ghost) cells, the
  * face slots per cell of the step kernels. */
 int  hcfd_gpu_info(hcfd_solver* s, int* Nc, int* Nf, int* Nreal, int* slots);
-/* Per-kernel timing with CUDA events on the handle's stream.  enable != 0 starts
- * recording every launch of the two step kernels; hcfd_gpu_profile_read returns the
- * summed milliseconds and launch counts since enabling. */
+/* Per-kernel timing with CUDA events on the handle's stream.  enable = N > 0 starts
+ * recording the two step kernels' launches of every N-th step (N > 1 keeps the events'
+ * own cost out of most steps); 0 stops.  hcfd_gpu_profile_read returns the summed
+ * milliseconds and launch counts of the recorded launches since enabling. */
 int  hcfd_gpu_profile(hcfd_solver* s, int enable);
 int  hcfd_gpu_profile_read(hcfd_solver* s, double* ms_pass1, long long* n_pass1,
                            double* ms_pass2, long long* n_pass2);
@@ -276,6 +303,11 @@ int  hcfd_arena_step(hcfd_arena* a, int nsteps);
 int  hcfd_arena_poll(hcfd_arena* a, int max, int* slots, hcfd_step_stats* stats, int* n);
 /* Copies one instance's state (prims != 0: primitive) to 4 host arrays of its Nc doubles. */
 int  hcfd_arena_fetch(hcfd_arena* a, int slot, int prims, double* const* out);
+/* An instance's exact snapshot (hcfd_gpu_checkpoint's format), and its restore into an
+ * admitted instance of the same mesh, for preempting a served solve and resuming it later
+ * (here or in another arena) with the same results. */
+int  hcfd_arena_checkpoint(hcfd_arena* a, int slot, const char* path);
+int  hcfd_arena_restore(hcfd_arena* a, int slot, const char* path);
 /* Retires an instance and frees its ranges for later admissions. */
 int  hcfd_arena_release(hcfd_arena* a, int slot);
 int  hcfd_arena_info(hcfd_arena* a, hcfd_arena_info_t* info);

@@ -13,13 +13,18 @@
 //    default (the reference hard-codes "../sols/<Layout>", src/Base/Euler.cpp:22) and
 //    creates nothing; set another prefix with set_output();
 //  - Limiter takes an optional kind (Barth-Jespersen, as the reference, or
-//    Venkatakrishnan) and Euler an optional time mode, precision and kernel choice.
+//    Venkatakrishnan) and Euler an optional time mode, precision and kernel choice;
+//  - run() writes its snapshots without stopping the steps: each is copied to one of two
+//    page-locked host buffers while the steps go on, and a writer thread writes the file
+//    (the reference converts and writes between steps, src/Base/Euler.cpp:99-103); Q holds
+//    the primitive state of the last step when run() returns.
 #pragma once
 #include "hcfd_gpu.h"
 
 #include <algorithm>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace GPU {
@@ -143,7 +148,11 @@ public:
             Q[v] = qbuf_[v].data();
         }
     }
-    ~Euler() { hcfd_gpu_destroy(solver_); }
+    ~Euler() {
+        if (writer_.joinable()) writer_.join();
+        for (auto& b : snapbuf_) if (!b.empty()) hcfd_host_unpin(b.data());
+        hcfd_gpu_destroy(solver_);
+    }
     Euler(const Euler&) = delete;
     Euler& operator=(const Euler&) = delete;
 
@@ -169,15 +178,41 @@ public:
     const int Nc, Nf, nvars;
 
 private:
+    // Snapshot k goes to buffer k % 2 (its last user, writer k - 2, was joined at output
+    // k - 1); the copy overlaps the wait for writer k - 1, then writer k takes over.
     void write_soln() {
-        static const char* names[4] = {"Density", "Velocity_X", "Velocity_Y", "Pressure"};
+        const int b = runcount_ % 2;
+        if (snapbuf_[b].empty()) {
+            snapbuf_[b].assign(4 * (size_t) Nc, 0.0);
+            check(hcfd_host_pin(snapbuf_[b].data(), sizeof(double) * snapbuf_[b].size()));
+        }
+        double* arrs[4];
+        for (int v = 0; v < 4; v++) arrs[v] = snapbuf_[b].data() + (size_t) v * Nc;
+        hcfd_snapshot* t = nullptr;
+        check(hcfd_gpu_snapshot(solver_, 1, arrs, &t));
+        join_writer();
         const std::string fn = prefix_ + "_" + std::to_string(runcount_++) + ".hsln";
-        const double* arrs[4] = {Q[0], Q[1], Q[2], Q[3]};
-        check(hcfd_write_hsln(fn.c_str(), 4, names, Nc, arrs));
+        const int nc = Nc;
+        writer_ = std::thread([this, t, fn, b, nc]() {
+            static const char* names[4] = {"Density", "Velocity_X", "Velocity_Y", "Pressure"};
+            const double* out[4];
+            for (int v = 0; v < 4; v++) out[v] = snapbuf_[b].data() + (size_t) v * nc;
+            int rc = hcfd_snapshot_wait(t);
+            if (rc == HCFD_OK) rc = hcfd_write_hsln(fn.c_str(), 4, names, nc, out);
+            if (rc != HCFD_OK) writer_error_ = std::string("hcfd: ") + hcfd_last_error();
+            hcfd_snapshot_free(t);
+        });
+    }
+    void join_writer() {
+        if (writer_.joinable()) writer_.join();
+        if (!writer_error_.empty()) {
+            const std::string e = writer_error_;
+            writer_error_.clear();
+            throw std::runtime_error(e);
+        }
     }
     void run_mode(double T, int mode, double value, double dt_out) {
         double t = 0.0, t_out = dt_out;
-        compute_prims();
         write_soln();
         if (mode == HCFD_FIXED_DT) {
             // the steps up to each output are counted with the reference's own t += dt
@@ -190,7 +225,6 @@ private:
                 }
                 check(hcfd_gpu_step(solver_, n, mode, value, nullptr));
                 if (t >= t_out) {
-                    compute_prims();
                     write_soln();
                     t_out += dt_out;
                 }
@@ -201,12 +235,13 @@ private:
                 check(hcfd_gpu_step(solver_, 1, mode, value, &st));
                 t += st.dt;
                 if (t >= t_out) {
-                    compute_prims();
                     write_soln();
                     t_out += dt_out;
                 }
             }
         }
+        join_writer();
+        compute_prims();
     }
 
     Domain& domain;
@@ -215,6 +250,9 @@ private:
     std::vector<double> qbuf_[4];
     std::string prefix_ = "../sols/GPU";
     int runcount_ = 0;
+    std::vector<double> snapbuf_[2];      // page-locked snapshot buffers, 4 x Nc each
+    std::thread writer_;
+    std::string writer_error_;
 };
 
 }  // namespace GPU
