@@ -1,0 +1,138 @@
+"""gmsh import and .vtu export on the CPU: a small mixed triangle/quadrangle mesh written as gmsh
+4.1 ASCII, imported to .hmsh, loaded by the library's checked reader and stepped by the oracle;
+solutions exported to .vtu and read back."""
+import base64
+import struct
+import xml.etree.ElementTree as ET
+
+import numpy as np
+import pytest
+
+import cfd_optimisations_b200 as H
+from cfd_optimisations_b200 import meshio
+import oracle as O
+
+
+def write_msh(path, nx=9, ny=5, tags=(1, 2, 3, 4), untagged_curve=None):
+    """Rectangle [0,2]x[0,1]: quadrangles in the left half, triangles in the right half;
+    curves bottom, right, top, left with physical tags `tags`, the surface with tag 9."""
+    xs, ys = np.linspace(0, 2, nx), np.linspace(0, 1, ny)
+    nid = lambda i, j: 1 + j * nx + i
+    nodes = [(nid(i, j), xs[i], ys[j]) for j in range(ny) for i in range(nx)]
+    quads, tris = [], []
+    for j in range(ny - 1):
+        for i in range(nx - 1):
+            a, b, c, d = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
+            if i < (nx - 1) // 2:
+                quads.append((a, b, c, d))
+            else:
+                tris += [(a, b, c), (a, c, d)]
+    sides = {1: [(nid(i, 0), nid(i + 1, 0)) for i in range(nx - 1)],
+             2: [(nid(nx - 1, j), nid(nx - 1, j + 1)) for j in range(ny - 1)],
+             3: [(nid(i + 1, ny - 1), nid(i, ny - 1)) for i in range(nx - 1)],
+             4: [(nid(0, j + 1), nid(0, j)) for j in range(ny - 1)]}
+    names = {1: "lower", 2: "outlet", 3: "upper", 4: "inlet"}
+    L = ["$MeshFormat", "4.1 0 8", "$EndMeshFormat", "$PhysicalNames", "5"]
+    for c in (1, 2, 3, 4):
+        L.append(f'1 {tags[c - 1]} "{names[c]}"')
+    L.append('2 9 "domain"')
+    L += ["$EndPhysicalNames", "$Entities", "4 4 1 0"]
+    for p in range(1, 5):
+        L.append(f"{p} 0 0 0 0")
+    for c in (1, 2, 3, 4):
+        ph = "0" if c == untagged_curve else f"1 {tags[c - 1]}"
+        L.append(f"{c} 0 0 0 2 1 0 {ph} 2 {c} {-(c % 4 + 1)}")
+    L.append("1 0 0 0 2 1 0 1 9 4 1 2 3 4")
+    L += ["$EndEntities", "$Nodes", f"1 {len(nodes)} 1 {len(nodes)}", f"2 1 0 {len(nodes)}"]
+    L += [str(t) for t, _, _ in nodes]
+    L += [f"{float(x)!r} {float(y)!r} 0" for _, x, y in nodes]
+    L.append("$EndNodes")
+    blocks, tag = [], 1
+    for c in (1, 2, 3, 4):
+        blocks.append((1, c, 1, sides[c]))
+    blocks += [(2, 1, 3, quads), (2, 1, 2, tris)]
+    nel = sum(len(b[3]) for b in blocks)
+    L += ["$Elements", f"{len(blocks)} {nel} 1 {nel}"]
+    for d, e, t, els in blocks:
+        L.append(f"{d} {e} {t} {len(els)}")
+        for el in els:
+            L.append(" ".join(str(x) for x in (tag,) + tuple(el)))
+            tag += 1
+    L.append("$EndElements")
+    with open(path, "w") as fh:
+        fh.write("\n".join(L) + "\n")
+    return dict(nquads=len(quads), ntris=len(tris), nlines=sum(len(v) for v in sides.values()))
+
+
+def test_import_builds_a_valid_mesh(tmp_path):
+    info = write_msh(tmp_path / "r.msh", tags=(3, 5, 7, 8))
+    m = meshio.import_msh(str(tmp_path / "r.msh"), str(tmp_path / "r.hmsh"))
+    nreal = info["nquads"] + info["ntris"]
+    assert m["Nc"] == nreal + info["nlines"]
+    mesh = H.Mesh(str(tmp_path / "r.hmsh"))          # the library's checked reader accepts it
+    a = mesh.arrays()
+    assert a["Nc"] == m["Nc"] and a["Nf"] == m["Nf"] and a["Ncol"] == 5 and a["NBCcol"] == 4
+    assert a["pnames"] == ["lower", "outlet", "upper", "inlet"]            # tags 3 < 5 < 7 < 8
+    fc = a["fc_con"].reshape(-1, 2)
+    ctypes = m["c_ctypes"]
+    F_BC = a["coloff"][1]
+    assert np.all(ctypes[fc[F_BC:, 1]] == 1) and np.all(ctypes[fc[F_BC:, 0]] != 1)   # ghosts on the right
+    assert np.all(ctypes[fc[:F_BC].ravel()] != 1) and np.all(fc[:F_BC, 0] < fc[:F_BC, 1])
+    assert np.all(np.diff(a["coloff"]) == [m["Nf"] - info["nlines"], 8, 4, 8, 4])
+    # every real cell has as many faces as sides
+    deg = np.bincount(fc.ravel(), minlength=m["Nc"])
+    assert np.all(deg[ctypes == 3] == 4) and np.all(deg[ctypes == 2] == 3) and np.all(deg[ctypes == 1] == 1)
+
+
+def test_imported_mesh_keeps_a_uniform_flow_uniform(tmp_path):
+    """Green-Gauss of a constant and the sum of a constant flux vanish on closed cells: the
+    oracle stepping a freestream on the imported mesh must leave it unchanged."""
+    write_msh(tmp_path / "r.msh")
+    meshio.import_msh(str(tmp_path / "r.msh"), str(tmp_path / "r.hmsh"))
+    mesh = H.Mesh(str(tmp_path / "r.hmsh"))
+    o = O.Oracle(mesh.arrays())
+    q = [1.4, 2.5, 0.3, 1.0]
+    o.gather_bcs([O.SYMMETRY, O.SUPINLET, O.SUPINLET, O.SUPINLET, O.SUPINLET], [q] * 4)
+    o.initialise(q)
+    U0 = o.U()
+    for _ in range(5):
+        o.step(O.FIXED_DT, 1e-3)
+    assert np.max(np.abs(o.U() - U0)) <= 1e-12 * np.max(np.abs(U0))
+
+
+def test_import_errors(tmp_path):
+    write_msh(tmp_path / "u.msh", untagged_curve=2)
+    with pytest.raises(meshio.MshError, match="no physical tag"):
+        meshio.import_msh(str(tmp_path / "u.msh"), str(tmp_path / "u.hmsh"))
+    (tmp_path / "v.msh").write_text("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n")
+    with pytest.raises(meshio.MshError, match="4.x ASCII"):
+        meshio.read_msh(str(tmp_path / "v.msh"))
+
+
+def decode(arr):
+    raw = base64.b64decode(arr.text)
+    n = struct.unpack_from("<I", raw)[0]
+    dt = {"Float64": np.float64, "Int64": np.int64, "UInt8": np.uint8}[arr.get("type")]
+    return np.frombuffer(raw[4:4 + n], dtype=dt)
+
+
+def test_export_vtu_round_trip(tmp_path):
+    write_msh(tmp_path / "r.msh")
+    m = meshio.import_msh(str(tmp_path / "r.msh"), str(tmp_path / "r.hmsh"))
+    rng = np.random.default_rng(1)
+    data = rng.normal(size=(4, m["Nc"]))
+    names = ["Density", "Velocity_X", "Velocity_Y", "Pressure"]
+    H.write_hsln(str(tmp_path / "s_3.hsln"), list(data), names)
+    meshio.main(["export", str(tmp_path / "r.hmsh"), str(tmp_path / "s_3.hsln"), str(tmp_path / "s.vtu")])
+    piece = ET.parse(tmp_path / "s.vtu").getroot().find("UnstructuredGrid/Piece")
+    assert int(piece.get("NumberOfCells")) == m["Nc"] and int(piece.get("NumberOfPoints")) == m["Nn"]
+    cells = {a.get("Name"): decode(a) for a in piece.find("Cells")}
+    assert np.array_equal(cells["connectivity"], m["cn_con"]) and np.array_equal(cells["offsets"], m["cn_off"][1:])
+    assert set(np.unique(cells["types"])) == {3, 5, 9}
+    cd = {a.get("Name"): decode(a) for a in piece.find("CellData")}
+    assert np.array_equal(cd["Density"], data[0]) and np.array_equal(cd["Pressure"], data[3])
+    vel = cd["Velocity"].reshape(-1, 3)
+    assert np.array_equal(vel[:, 0], data[1]) and np.array_equal(vel[:, 1], data[2]) and not vel[:, 2].any()
+    out = meshio.batch_export(str(tmp_path / "r.hmsh"), str(tmp_path / "s_%d.hsln"), str(tmp_path / "o_%d.vtu"))
+    assert out == [str(tmp_path / "o_3.vtu")]
+    assert meshio.check_cell(str(tmp_path / "r.hmsh"), 0)["cell"] == 0
