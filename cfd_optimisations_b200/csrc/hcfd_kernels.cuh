@@ -151,13 +151,31 @@ __device__ __forceinline__ void st_grad(Grad8<float>* p, size_t ps, int i, const
 }
 
 // ---------------------------------------------------------------------------------------
+// Reciprocals, quotients and square roots of the step arithmetic.  FP64 keeps the IEEE
+// operations (bit parity with the reference needs them); FP32 uses the hardware
+// approximations (a few units in the last place), since nothing compares FP32 bit for bit and
+// the IEEE sequences would cost a fair share of the FP32 kernels' issue slots.
+template <class T>
+__device__ __forceinline__ T qrcp(T x) { return T(1) / x; }
+template <>
+__device__ __forceinline__ float qrcp<float>(float x) { return __fdividef(1.0f, x); }
+template <class T>
+__device__ __forceinline__ T qdiv(T a, T b) { return a / b; }
+template <>
+__device__ __forceinline__ float qdiv<float>(float a, float b) { return __fdividef(a, b); }
+template <class T>
+__device__ __forceinline__ T qsqrt(T x) { return sqrt(x); }
+template <>
+__device__ __forceinline__ float qsqrt<float>(float x) { return x == 0.0f ? 0.0f : x * rsqrtf(x); }
+
+// ---------------------------------------------------------------------------------------
 // flux arithmetic, written with the reference's expression trees
 
 // Flux::EulerFlux (src/Base/Flux.cpp:89-97).
 template <class T>
 __device__ __forceinline__ void euler_flux(const T U[4], T n0, T n1, T gma, T F[4]) {
     const T gmo = gma - T(1);
-    const T ir = T(1) / U[0];
+    const T ir = qrcp(U[0]);
     const T P = gmo * (U[3] - T(0.5) * ir * (U[1] * U[1] + U[2] * U[2]));
     F[0] = n0 * U[1] + n1 * U[2];
     F[1] = n0 * (U[1] * U[1] * ir + P) + n1 * U[2] * U[1] * ir;
@@ -169,16 +187,16 @@ __device__ __forceinline__ void euler_flux(const T U[4], T n0, T n1, T gma, T F[
 template <class T>
 __device__ __forceinline__ void rusanov(const T UL[4], const T UR[4], T n0, T n1, T gma, T F[4]) {
     const T gmo = gma - T(1);
-    const T irl = T(1) / UL[0];
-    const T irr = T(1) / UR[0];
+    const T irl = qrcp(UL[0]);
+    const T irr = qrcp(UR[0]);
     const T nvl = (n0 * UL[1] + n1 * UL[2]) * irl;
     const T nvr = (n0 * UR[1] + n1 * UR[2]) * irr;
     const T qql = T(0.5) * (UL[1] * UL[1] + UL[2] * UL[2]) * irl;
     const T qqr = T(0.5) * (UR[1] * UR[1] + UR[2] * UR[2]) * irr;
     const T pl = gmo * (UL[3] - qql);
     const T pr = gmo * (UR[3] - qqr);
-    const T al = sqrt(gma * pl * irl);
-    const T ar = sqrt(gma * pr * irr);
+    const T al = qsqrt(gma * pl * irl);
+    const T ar = qsqrt(gma * pr * irr);
     const T S1 = fmax(fabs(nvl - al), fabs(nvr - ar));
     const T S2 = fmax(fabs(nvl + al), fabs(nvr + ar));
     const T S = fmax(S1, S2);
@@ -198,11 +216,11 @@ __device__ __forceinline__ T wave(T u, T v, T a, const FaceGeo<T>& g) {
 
 template <class T>
 __device__ __forceinline__ void cell_speed(const T U[4], T gma, T& u, T& v, T& a) {
-    const T ir = T(1) / U[0];
+    const T ir = qrcp(U[0]);
     u = U[1] * ir;
     v = U[2] * ir;
     const T p = (gma - T(1)) * (U[3] - T(0.5) * (U[1] * u + U[2] * v));
-    a = sqrt(gma * p * ir);
+    a = qsqrt(gma * p * ir);
 }
 
 // Venkatakrishnan face limiter for one side: min(1, (D1^2 + e2 + 2 D1 d)/(D1^2 + 2 d^2 +
@@ -211,7 +229,7 @@ template <class T>
 __device__ __forceinline__ T venkat(T D1, T d, T e2) {
     const T num = D1 * D1 + e2 + T(2) * D1 * d;
     const T den = D1 * D1 + T(2) * d * d + D1 * d + e2;
-    return fmin(T(1), num / den);
+    return fmin(T(1), qdiv(num, den));
 }
 
 // Two-sum accumulation s + c += x (Knuth), with explicit round-to-nearest adds so that no
@@ -330,7 +348,7 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
             }
             T e2 = T(0);
             if (a.limiter == LIM_VENKAT) {
-                const T kh = a.venkat_K * sqrt(T(1) / iv);
+                const T kh = a.venkat_K * qsqrt(qrcp(iv));
                 e2 = kh * kh * kh;
             }
             const T eps = T(1e-9);
@@ -351,7 +369,7 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
                         T pf = T(1);
                         if (a.limiter == LIM_BJ) {                   // Limiter.cpp:67-71
                             // one division: the numerator is picked by the sign of d
-                            if (d > eps || d < -eps) pf = fmin(T(1), ((d > eps) ? umax[v] - u[v] : umin[v] - u[v]) / d);
+                            if (d > eps || d < -eps) pf = fmin(T(1), qdiv((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d));
                         } else {
                             if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
                         }
@@ -364,7 +382,7 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
             }
             if (lmode == LIM_RECORD) st_cell(a.phiF, a.Nc, c, phis);
             st_grad(a.phiG, a.Nc, c, out);
-            if (a.time_mode != TM_FIXED) dtc = (double) (T(1) / (iv * lam));
+            if (a.time_mode != TM_FIXED) dtc = (double) qrcp(iv * lam);
         }
     }
     if (a.time_mode != TM_FIXED) {
@@ -453,7 +471,7 @@ __global__ void __launch_bounds__(256) pass2_kernel(const StepArgs<T> a) {
                 if (a.time_mode == TM_LOCAL) lam += wave(cu, cv, ca, g);
             }
             T dt;
-            if (a.time_mode == TM_LOCAL) dt = T(a.dt_or_cfl) * (T(1) / (iv * lam));
+            if (a.time_mode == TM_LOCAL) dt = T(a.dt_or_cfl) * qrcp(iv * lam);
             else dt = T(dt_used);
             T un_[4];
 #pragma unroll

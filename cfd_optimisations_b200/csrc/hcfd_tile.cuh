@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
         }
         T e2 = T(0);
         if (s.limiter == LIM_VENKAT) {
-            const T kh = s.venkat_K * sqrt(T(1) / iv);
+            const T kh = s.venkat_K * qsqrt(qrcp(iv));
             e2 = kh * kh * kh;
         }
         const T eps = T(1e-9);
@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
                     T pf = T(1);
                     if (s.limiter == LIM_BJ) {                       // Limiter.cpp:67-71
                         // one division: the numerator is picked by the sign of d
-                        if (d > eps || d < -eps) pf = fmin(T(1), ((d > eps) ? umax[v] - u[v] : umin[v] - u[v]) / d);
+                        if (d > eps || d < -eps) pf = fmin(T(1), qdiv((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d));
                     } else {
                         if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
                     }
@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
         }
         if (lmode == LIM_RECORD) st_cell(s.phiF, a.ps, base + c, phis);
         st_grad(s.phiG, a.ps, base + c, out);
-        if (s.time_mode != TM_FIXED) dtc = fmin(dtc, (double) (T(1) / (iv * lam)));
+        if (s.time_mode != TM_FIXED) dtc = fmin(dtc, (double) qrcp(iv * lam));
     }
     if constexpr (ARENA) {
         // per-instance minimum (exact and order-free): each warp carries its minimum across
@@ -593,7 +593,7 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
             }
         }
         T dt;
-        if (s.time_mode == TM_LOCAL) dt = cfl_or_dt * (T(1) / (iv * lam));
+        if (s.time_mode == TM_LOCAL) dt = cfl_or_dt * qrcp(iv * lam);
         else dt = T(dt_used);
         T un_[4];
 #pragma unroll
