@@ -193,6 +193,18 @@ struct hcfd_arena {
     cudaStream_t stream = nullptr;
     int B = 128, W = 3, Wp = 4, Hcap = 112, Fcap = 288;   // staging capacities (admission limit)
     int Hcur = 0, Fcur = 0;                               // largest halo / entries of the active tiles
+    bool dirty = false;                                   // the active list changed since the last rebuild
+    // Admissions upload and compute on their own stream, so that they overlap the steps of
+    // the instances already active; the step stream waits for them (admit_ev) only when the
+    // new instances join the active list.
+    cudaStream_t astream = nullptr;
+    cudaEvent_t admit_ev = nullptr;
+    bool admit_pending = false;
+    // host copies of the last active-list upload and the event after which they may change
+    std::vector<int> tl_host;
+    std::vector<int4> act_host;
+    cudaEvent_t list_ev = nullptr;
+    bool list_pending = false;
     size_t Ccap = 0, Ecap = 0, HLcap = 0;
     FreeList fc, fe, fh;
     size_t tsz = 8;
@@ -245,6 +257,15 @@ namespace {
 
 void free_graph(hcfd_arena* a) {
     if (a->graph) { cudaGraphExecDestroy(a->graph); a->graph = nullptr; a->graph_steps = 0; }
+}
+
+// Orders the step stream after every admission enqueued so far (device-side wait).
+int wait_admissions(hcfd_arena* A) {
+    if (A->admit_pending) {
+        CK(cudaStreamWaitEvent(A->stream, A->admit_ev, 0));
+        A->admit_pending = false;
+    }
+    return HCFD_OK;
 }
 
 template <class T>
@@ -340,8 +361,14 @@ int configure(hcfd_arena* A) {
 
 // Rebuilds the active tile list and the per-instance tile ranges, in slot order.
 int rebuild_active(hcfd_arena* A) {
-    std::vector<int> tl;
-    std::vector<int4> act;
+    int rc = wait_admissions(A);
+    if (rc) return rc;
+    // the previous upload must have read the host copies before they change
+    if (A->list_pending) CK(cudaEventSynchronize(A->list_ev));
+    std::vector<int>& tl = A->tl_host;
+    std::vector<int4>& act = A->act_host;
+    tl.clear();
+    act.clear();
     int hmax = 0, fmax = 4;
     for (size_t k = 0; k < A->inst.size(); k++) {
         const Inst& I = A->inst[k];
@@ -355,12 +382,15 @@ int rebuild_active(hcfd_arena* A) {
     A->nact_tiles = (int) (tl.size() / 8);
     A->nact = (int) act.size();
     if ((size_t) A->nact_tiles > A->tiles_cap) return fail(HCFD_EINVAL, "arena: tile list capacity exceeded");
+    // stream-ordered after the steps already enqueued, before the next ones
     if (!tl.empty()) CK(cudaMemcpyAsync(A->tiles, tl.data(), sizeof(int) * tl.size(), cudaMemcpyHostToDevice, A->stream));
     if (!act.empty()) CK(cudaMemcpyAsync(A->act, act.data(), sizeof(int4) * act.size(), cudaMemcpyHostToDevice, A->stream));
-    CK(cudaStreamSynchronize(A->stream));
+    CK(cudaEventRecord(A->list_ev, A->stream));
+    A->list_pending = true;
     free_graph(A);
     A->Hcur = hmax;
     A->Fcur = fmax;
+    A->dirty = false;
     return configure(A);
 }
 
@@ -377,9 +407,13 @@ int dalloc(P** p, size_t n) {
 void arena_free(hcfd_arena* A) {
     if (!A) return;
     cudaSetDevice(A->device);
+    if (A->astream) cudaStreamSynchronize(A->astream);
     if (A->stream) cudaStreamSynchronize(A->stream);
     free_graph(A);
     for (auto& I : A->inst) if (I.d_perm) cudaFree(I.d_perm);
+    if (A->admit_ev) cudaEventDestroy(A->admit_ev);
+    if (A->list_ev) cudaEventDestroy(A->list_ev);
+    if (A->astream) cudaStreamDestroy(A->astream);
     void* p[] = {A->U[0], A->U[1], A->phiG, A->phiF, A->iv, A->cslot, A->tgeo, A->tmeta, A->halo, A->inst_dt, A->inst_dtmin,
                  A->inst_bc, A->stats, A->tiles, A->act, A->tile_r2, A->tile_bad, A->err};
     for (void* q : p) if (q) cudaFree(q);
@@ -440,6 +474,9 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
     A->fh.init(A->HLcap);
     A->inst.resize(p.max_instances);
     CK(cudaStreamCreateWithFlags(&A->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&A->astream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&A->admit_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&A->list_ev, cudaEventDisableTiming));
     hcfd_arena* h = A.get();
     auto bail = [&](int code) { arena_free(h); A.release(); delete h; return code; };
     int rc;
@@ -562,7 +599,7 @@ int hcfd_arena_admit_prepared(hcfd_arena* A, const hcfd_admission* D, int* slot_
         d[6] = d[7] = 0;
     }
     // device work: geometry of this mesh (stream-ordered temporaries), then the arena ranges
-    cudaStream_t st = A->stream;
+    cudaStream_t st = A->astream;
     int *d_fn = nullptr, *d_fcu = nullptr, *d_fcg = nullptr, *d_cnoff = nullptr, *d_cncon = nullptr, *d_cfoff = nullptr,
         *d_cfcon = nullptr, *d_efid = nullptr, *d_foff = nullptr, *d_iperm = nullptr, *d_halo = nullptr;
     double *d_nodes = nullptr, *d_xc = nullptr, *d_ivu = nullptr;
@@ -581,10 +618,10 @@ int hcfd_arena_admit_prepared(hcfd_arena* A, const hcfd_admission* D, int* slot_
                      d_nodes, d_xc, d_ivu, d_geo};
         for (void* q : t) if (q) cudaFreeAsync(q, st);
     };
-    if (ce == cudaSuccess) ce = cudaMalloc((void**) &I.d_perm, sizeof(int) * (size_t) Nc);
+    if (ce == cudaSuccess) ce = cudaMallocAsync((void**) &I.d_perm, sizeof(int) * (size_t) Nc, st);
     if (ce != cudaSuccess) {
         tmp_free();
-        if (I.d_perm) cudaFree(I.d_perm);
+        if (I.d_perm) cudaFreeAsync(I.d_perm, st);
         cudaStreamSynchronize(st);
         undo();
         return fail(ce == cudaErrorMemoryAllocation ? HCFD_ENOMEM : HCFD_ECUDA,
@@ -643,20 +680,22 @@ int hcfd_arena_admit_prepared(hcfd_arena* A, const hcfd_admission* D, int* slot_
     up(A->inst_bc + slot, &D->bc, sizeof(hcfd::BCTable));
     if (ce == cudaSuccess) ce = cudaMemsetAsync(A->stats + slot, 0, sizeof(hcfd::StepStats), st);
     tmp_free();
-    // the uploads above read pageable host memory (the stack included): wait for them
-    const cudaError_t se = cudaStreamSynchronize(st);
-    if (ce == cudaSuccess) ce = se;
+    // Host sources are pageable (the stack included): each upload has copied its source by the
+    // time it returns.  The device work goes on behind the steps already enqueued; the step
+    // stream waits for it when the active list next changes.
+    if (ce == cudaSuccess) ce = cudaEventRecord(A->admit_ev, st);
     if (ce != cudaSuccess) {
+        cudaStreamSynchronize(st);
         cudaFree(I.d_perm);
         undo();
         return fail(HCFD_ECUDA, std::string("arena_admit: ") + cudaGetErrorString(ce));
     }
+    A->admit_pending = true;
     I.dt = D->dt;
     I.active = true;
     I.admitted_step = A->steps_done;
     A->inst[slot] = std::move(I);
-    int rc = rebuild_active(A);
-    if (rc) return rc;
+    A->dirty = true;     // the active list is rebuilt once before the next step, however many are admitted
     *slot_out = slot;
     return HCFD_OK;
 }
@@ -675,6 +714,10 @@ int hcfd_arena_step(hcfd_arena* A, int nsteps) {
     hcfd::clear_error();
     if (!A || nsteps < 0) return fail(HCFD_EINVAL, "arena_step: bad argument");
     CK(cudaSetDevice(A->device));
+    if (A->dirty) {
+        const int rc = rebuild_active(A);
+        if (rc) return rc;
+    }
     if (A->nact == 0 || nsteps == 0) return HCFD_OK;
     // one graph holds two steps (the ping-pong buffers and dt slots return to their start)
     if (!A->graph) {
@@ -711,6 +754,10 @@ int hcfd_arena_poll(hcfd_arena* A, int max, int* slots, hcfd_step_stats* stats, 
     hcfd::clear_error();
     if (!A || !n || max < 0 || (max > 0 && (!slots || !stats))) return fail(HCFD_EINVAL, "arena_poll: bad argument");
     CK(cudaSetDevice(A->device));
+    {
+        const int rc_ = wait_admissions(A);
+        if (rc_) return rc_;
+    }
     std::vector<hcfd::StepStats> st(A->inst.size());
     unsigned int err = 0;
     CK(cudaMemcpyAsync(st.data(), A->stats, sizeof(hcfd::StepStats) * st.size(), cudaMemcpyDeviceToHost, A->stream));
@@ -738,6 +785,10 @@ int hcfd_arena_fetch(hcfd_arena* A, int slot, int prims, double* const* out) {
     if (!A || slot < 0 || slot >= (int) A->inst.size() || !A->inst[slot].active || !out)
         return fail(HCFD_EINVAL, "arena_fetch: bad argument");
     CK(cudaSetDevice(A->device));
+    {
+        const int rc_ = wait_admissions(A);
+        if (rc_) return rc_;
+    }
     const Inst& I = A->inst[slot];
     double* d_out = nullptr;
     CK(cudaMallocAsync((void**) &d_out, sizeof(double) * 4 * (size_t) I.Nc, A->stream));
@@ -760,6 +811,10 @@ int hcfd_arena_checkpoint(hcfd_arena* A, int slot, const char* path) {
     if (!A || slot < 0 || slot >= (int) A->inst.size() || !A->inst[slot].active || !path)
         return fail(HCFD_EINVAL, "arena_checkpoint: bad argument");
     CK(cudaSetDevice(A->device));
+    {
+        const int rc_ = wait_admissions(A);
+        if (rc_) return rc_;
+    }
     const Inst& I = A->inst[slot];
     const size_t n = 4 * (size_t) I.Nc;
     const bool frz = A->phiF != nullptr;
@@ -803,6 +858,10 @@ int hcfd_arena_restore(hcfd_arena* A, int slot, const char* path) {
     if (!A || slot < 0 || slot >= (int) A->inst.size() || !A->inst[slot].active || !path)
         return fail(HCFD_EINVAL, "arena_restore: bad argument");
     CK(cudaSetDevice(A->device));
+    {
+        const int rc_ = wait_admissions(A);
+        if (rc_) return rc_;
+    }
     const Inst& I = A->inst[slot];
     hcfd::CkptHeader h;
     std::vector<double> U, phi;
@@ -842,6 +901,10 @@ int hcfd_arena_release(hcfd_arena* A, int slot) {
     hcfd::clear_error();
     if (!A || slot < 0 || slot >= (int) A->inst.size() || !A->inst[slot].active) return fail(HCFD_EINVAL, "arena_release: bad slot");
     CK(cudaSetDevice(A->device));
+    {
+        const int rc_ = wait_admissions(A);
+        if (rc_) return rc_;
+    }
     CK(cudaStreamSynchronize(A->stream));
     Inst& I = A->inst[slot];
     A->fc.release(I.c0 / A->B, I.ntiles);
@@ -849,11 +912,17 @@ int hcfd_arena_release(hcfd_arena* A, int slot) {
     A->fh.release(I.h0, I.nh);
     if (I.d_perm) cudaFree(I.d_perm);
     I = Inst();
-    return rebuild_active(A);
+    A->dirty = true;
+    return HCFD_OK;
 }
 
 int hcfd_arena_info(hcfd_arena* A, hcfd_arena_info_t* info) {
     if (!A || !info) return fail(HCFD_EINVAL, "arena_info: bad argument");
+    if (A->dirty) {
+        CK(cudaSetDevice(A->device));
+        const int rc = rebuild_active(A);
+        if (rc) return rc;
+    }
     info->cell_capacity = A->Ccap;
     info->cells_used = A->fc.used * A->B;
     info->face_capacity = A->Ecap;
