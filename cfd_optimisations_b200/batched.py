@@ -87,6 +87,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-loop", action="store_true", help="skip the FP64 loop baseline")
+    ap.add_argument("--tile", type=int, default=0, help="arena tile size (0: autotuned for the median instance)")
     a = ap.parse_args()
     specs = instance_specs(a.instances, a.seed)
     t0 = time.perf_counter()
@@ -94,7 +95,7 @@ def main():
     t_gen = time.perf_counter() - t0
     real = [m.Nc - (2 * (s["nx"] - 1) + 2 * (s["ny"] - 1)) for m, s in zip(meshes, specs)]
     median = int(np.median(real))
-    tile = autotune.best_arena_tile(median, FP32, LIMITER_BJ)
+    tile = a.tile or autotune.best_arena_tile(median, FP32, LIMITER_BJ)
     arena, slots, stats, t_admit, t_run = run_arena(meshes, specs, a.steps, tile=tile)
     upd = sum(real) * (a.steps - 2)
     out = dict(workload=dict(instances=a.instances, steps=a.steps, triangles_total=int(sum(real)),

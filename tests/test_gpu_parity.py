@@ -248,3 +248,21 @@ def test_imported_mixed_mesh_matches_oracle(tmp_path, kernel):
         dt_o, res_o = o.step(O.GLOBAL_CFL, 0.5)
         assert abs(st["dt"] - dt_o) <= 1e-13 * dt_o
     assert np.all(O.rel_linf(s.U(), o.U()) <= 1e-11)
+
+
+def test_config1_2000_steps_match_the_reference(tmp_path):
+    """The reference's CPU case, end to end: the 161 x 81 wedge (25,600 triangles, random
+    numbering), M 2.5, 15 deg, Barth-Jespersen, global CFL 0.5, 2000 steps on the GPU; the
+    reference (compiled unchanged) steps the same mesh with the GPU's dt sequence (it has no CFL
+    control of its own)."""
+    if not O.RefSolver.available():
+        pytest.skip("the reference library was not built here")
+    m = H.Mesh.wedge(161, 81, theta_deg=15.0, seed=1234, numbering=H.NUMBER_RANDOM)
+    path = str(tmp_path / "c1.hmsh")
+    m.write(path)
+    bcmap, qbc, q = H.wedge_case(2.5)
+    s = solver_for(m, bcmap, qbc, q)
+    dts = np.array([s.step(1, H.GLOBAL_CFL, 0.5)["dt"] for _ in range(2000)])
+    ref = O.RefSolver(path, bcmap, qbc, q)
+    ref.steps(2000, dts)
+    assert np.all(O.rel_linf(s.U(), ref.U()) <= MANY_STEPS)

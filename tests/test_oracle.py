@@ -85,6 +85,24 @@ def test_oracle_matches_reference_on_generated_meshes(tmp_path, numbering):
 
 
 @pytest.mark.skipif(not O.RefSolver.available(), reason="reference not compiled into oracle/_ref")
+def test_oracle_matches_reference_on_the_config1_wedge(tmp_path):
+    """The 161 x 81 wedge of the reference's CPU case, Barth-Jespersen, global CFL 0.5: the
+    reference stepped with the oracle's dt sequence stays bit-identical (200 steps here; 2000
+    in the GPU suite against the GPU solver)."""
+    m = H.Mesh.wedge(161, 81, theta_deg=15.0, seed=1234, numbering=H.NUMBER_RANDOM)
+    path = str(tmp_path / "c1.hmsh")
+    m.write(path)
+    bcmap, qbc, q = H.wedge_case(2.5)
+    o = O.Oracle(O.read_hmsh(path))
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    dts = [o.step(O.GLOBAL_CFL, 0.5)[0] for _ in range(200)]
+    r = O.RefSolver(path, bcmap, qbc, q)
+    r.steps(200, np.array(dts))
+    assert np.array_equal(o.U(), r.U())
+
+
+@pytest.mark.skipif(not O.RefSolver.available(), reason="reference not compiled into oracle/_ref")
 def test_oracle_phases_match_reference_phases(golden):
     """Gradient, limiter and residual arrays, phase by phase (Euler.cpp:86-96)."""
     path = os.path.join(golden, "wedge.hmsh")
