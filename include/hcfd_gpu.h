@@ -288,8 +288,11 @@ int  hcfd_arena_admit(hcfd_arena* a, const hcfd_mesh_view* mesh, const int* bcma
  * threads while another thread steps the arena.  hcfd_arena_prepare does the host work
  * (cell->face table, Morton order, tile plan, BC table); it reads only the arena's fixed
  * parameters, so any number of threads may call it at once.  The mesh arrays must stay
- * valid until the admission is freed.  hcfd_arena_admit_prepared claims the ranges, uploads
- * and activates; on HCFD_EAGAIN the admission stays valid for a later try. */
+ * valid until the admission is freed.  hcfd_arena_admit_prepared claims the ranges and
+ * enqueues the uploads and the set-up kernels on the arena's admission stream, behind which
+ * the steps already enqueued keep running; the instance joins the active set at the next
+ * hcfd_arena_step (poll, fetch, checkpoint, restore and release wait for pending admissions
+ * on the device).  On HCFD_EAGAIN the admission stays valid for a later try. */
 typedef struct hcfd_admission hcfd_admission;
 int  hcfd_arena_prepare(const hcfd_arena* a, const hcfd_mesh_view* mesh, const int* bcmap, int nbcmap,
                         const double* qbc, const double* qic, double dt_or_cfl, hcfd_admission** out);
