@@ -238,6 +238,8 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="arena tile size (0: autotuned for the median request)")
     ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--baseline-sample", type=int, default=24)
+    ap.add_argument("--max-instances", type=int, default=65536,
+                    help="resident instance slots (admission is by the HBM budget below this cap)")
     a = ap.parse_args()
 
     from . import autotune
@@ -252,7 +254,7 @@ def main():
     k = max(1, len(reqs) // max(1, a.baseline_sample))
     sample = set(r.rid for r in reqs[::k][:a.baseline_sample])
     arena = Arena(budget, precision=FP32, limiter=LIMITER_BJ, time_mode=GLOBAL_CFL, tile=tile,
-                  max_instances=4096)
+                  max_instances=a.max_instances)
     srv = Server(arena, a.cfl, a.orders, a.max_steps, a.chunk, workers=a.workers, keep=lambda rid: rid in sample)
     t0 = time.perf_counter()
     res = srv.run(reqs)
@@ -265,7 +267,7 @@ def main():
                       "clipped [5e3, 2e6]", mach="U[1.8,4.0]", theta_deg="U[5,15]", stop=f"{a.orders} orders or "
                       f"{a.max_steps} steps", chunk=a.chunk, limiter="barth-jespersen", cfl=a.cfl,
                       time_mode="global per instance"),
-        served=dict(precision="fp32-compensated", tile=tile, budget_bytes=budget, wall_s=wall, makespan_s=span,
+        served=dict(precision="fp32-compensated", tile=tile, budget_bytes=budget, max_instances=a.max_instances, wall_s=wall, makespan_s=span,
                     solves_per_s=len(res) / span, latency_s=percentiles(lat),
                     queue_s=percentiles([r.t_admit - r.t_arrive for r in res]),
                     converged=sum(r.converged for r in res), failed=sum(r.failed for r in res),
