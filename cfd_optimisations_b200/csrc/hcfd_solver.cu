@@ -107,6 +107,11 @@ struct hcfd_solver {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t snap_free = nullptr;
     bool snap_used = false;
+    // two steps captured as one CUDA graph (the ping-pong buffers and dt slots return to
+    // their start), replayed while the time mode, dt/CFL value and buffer parity stay the same
+    cudaGraphExec_t graph = nullptr;
+    int g_mode = -1, g_cur = -1;
+    double g_value = 0.0;
     bool prof = false;
     int prof_every = 1;                  // record every prof_every-th step
     long long prof_count = 0;
@@ -132,6 +137,7 @@ void free_all(hcfd_solver* s) {
         void* q[] = {P.d_tgeo, P.d_tmeta, P.d_foff, P.d_hoff, P.d_halo, P.d_cslot, P.d_efid};
         for (void* p : q) if (p) cudaFree(p);
     }
+    if (s->graph) cudaGraphExecDestroy(s->graph);
     if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     if (s->d_snap) cudaFree(s->d_snap);
     if (s->snap_free) cudaEventDestroy(s->snap_free);
@@ -616,7 +622,34 @@ int hcfd_gpu_step(hcfd_solver* s, int nsteps, int time_mode, double dt_or_cfl, h
     if (!s->initialised) return fail(HCFD_EINVAL, "step: call initialise first");
     if (nsteps < 0 || time_mode < HCFD_FIXED_DT || time_mode > HCFD_LOCAL_CFL || !std::isfinite(dt_or_cfl) || dt_or_cfl < 0)
         return fail(HCFD_EINVAL, "step: bad argument");
-    for (int i = 0; i < nsteps; i++) {
+    int n = nsteps;
+    if (n >= 2 && !s->prof) {
+        if (s->graph && (s->g_mode != time_mode || s->g_value != dt_or_cfl || s->g_cur != s->cur)) {
+            cudaGraphExecDestroy(s->graph);
+            s->graph = nullptr;
+        }
+        if (!s->graph) {
+            const int cur0 = s->cur;
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < 2 && rc == HCFD_OK; k++)
+                rc = s->fp32() ? launch_step_w<float>(s, time_mode, dt_or_cfl) : launch_step_w<double>(s, time_mode, dt_or_cfl);
+            const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+            if (rc) return rc;
+            if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("step: capture: ") + cudaGetErrorString(e));
+            const cudaError_t ei = cudaGraphInstantiate(&s->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) {
+                s->graph = nullptr;
+                return fail(HCFD_ECUDA, std::string("step: instantiate: ") + cudaGetErrorString(ei));
+            }
+            s->g_mode = time_mode;
+            s->g_value = dt_or_cfl;
+            s->g_cur = cur0;   // the capture flipped cur twice: back where it started
+        }
+        for (; n >= 2; n -= 2) CK(cudaGraphLaunch(s->graph, s->stream));
+    }
+    for (; n > 0; n--) {
         rc = s->fp32() ? launch_step_w<float>(s, time_mode, dt_or_cfl) : launch_step_w<double>(s, time_mode, dt_or_cfl);
         if (rc) return rc;
     }
