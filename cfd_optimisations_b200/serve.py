@@ -194,6 +194,43 @@ class Server:
         return sorted(results, key=lambda x: x.rid)
 
 
+def partition(reqs: list[Request], ndev: int) -> list[list[Request]]:
+    """Replicas over several GPUs: each request, in arrival order, goes to the device with the
+    fewest triangles assigned so far (its arena's memory and work grow with them)."""
+    loads = [0] * ndev
+    parts = [[] for _ in range(ndev)]
+    for r in sorted(reqs, key=lambda r: r.t_arrive):
+        d = min(range(ndev), key=lambda i: (loads[i], i))
+        parts[d].append(r)
+        loads[d] += r.triangles
+    return parts
+
+
+def serve_devices(reqs: list[Request], make_server, devices) -> tuple[list[Result], list[list[Request]]]:
+    """One Server with its own arena per device, each in its own thread (the thread's current
+    device is the one it serves); no data crosses devices.  `make_server(device)` builds the
+    server in that thread.  Returns all results by request id and the partition."""
+    import threading
+    parts = partition(reqs, len(devices))
+    out = [None] * len(devices)
+    errors = []
+
+    def work(i, dev):
+        try:
+            out[i] = make_server(dev).run(parts[i]) if parts[i] else []
+        except BaseException as e:          # reported after all threads end
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(i, d)) for i, d in enumerate(devices)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return sorted((r for part in out for r in part), key=lambda r: r.rid), parts
+
+
 def solve_alone_fp64(r: Request, cfl: float, orders: float, max_steps: int, chunk: int, rho_scale: float = 1.0,
                      **kw):
     """One request through the plain FP64 solver; returns (device ms, Result-like dict, U).
@@ -238,6 +275,7 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="arena tile size (0: autotuned for the median request)")
     ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--baseline-sample", type=int, default=24)
+    ap.add_argument("--devices", type=int, default=1, help="GPUs, one arena each (replicas, no collective)")
     ap.add_argument("--max-instances", type=int, default=65536,
                     help="resident instance slots (admission is by the HBM budget below this cap)")
     a = ap.parse_args()
@@ -253,12 +291,21 @@ def main():
     tile = a.tile or autotune.best_arena_tile(med, FP32, LIMITER_BJ)
     k = max(1, len(reqs) // max(1, a.baseline_sample))
     sample = set(r.rid for r in reqs[::k][:a.baseline_sample])
-    arena = Arena(budget, precision=FP32, limiter=LIMITER_BJ, time_mode=GLOBAL_CFL, tile=tile,
-                  max_instances=a.max_instances)
-    srv = Server(arena, a.cfl, a.orders, a.max_steps, a.chunk, workers=a.workers, keep=lambda rid: rid in sample)
+    servers = []
+
+    def make_server(dev):
+        from . import set_device
+        set_device(dev)
+        arena = Arena(budget, precision=FP32, limiter=LIMITER_BJ, time_mode=GLOBAL_CFL, tile=tile,
+                      max_instances=a.max_instances)
+        srv = Server(arena, a.cfl, a.orders, a.max_steps, a.chunk, workers=a.workers, keep=lambda rid: rid in sample)
+        servers.append(srv)
+        return srv
+
     t0 = time.perf_counter()
-    res = srv.run(reqs)
+    res, _ = serve_devices(reqs, make_server, list(range(a.devices)))
     wall = time.perf_counter() - t0
+    busy = sum(srv.busy_s for srv in servers) / len(servers)
     span = max(r.t_done for r in res)
     lat = [r.latency for r in res]
     cell_steps = sum(r.triangles * r.steps for r in res)
@@ -272,8 +319,11 @@ def main():
                     queue_s=percentiles([r.t_admit - r.t_arrive for r in res]),
                     converged=sum(r.converged for r in res), failed=sum(r.failed for r in res),
                     steps=percentiles([r.steps for r in res]), cell_updates_per_s=cell_steps / span,
-                    device_busy_fraction=srv.busy_s / span, max_active=srv.max_active, max_cells=srv.max_cells))
-    del arena
+                    devices=a.devices, device_busy_fraction=busy / span,
+                    max_active=max(srv.max_active for srv in servers), max_cells=max(srv.max_cells for srv in servers)))
+    for srv in servers:
+        del srv.arena
+    servers.clear()
     # baseline on the sample
     base, errs, errs64 = [], [], []
     for r in reqs:

@@ -137,3 +137,31 @@ def test_server_rejects_request_larger_than_arena():
 def test_max_steps_multiple_of_chunk():
     with pytest.raises(ValueError):
         serve.Server(FakeArena(1, {}), max_steps=1000, chunk=300)
+
+
+def test_partition_balances_triangles():
+    reqs = serve.request_stream(200, 100.0, 4)
+    parts = serve.partition(reqs, 3)
+    assert sorted(r.rid for p in parts for r in p) == list(range(200))
+    loads = [sum(r.triangles for r in p) for p in parts]
+    assert max(loads) - min(loads) <= max(r.triangles for r in reqs)
+    assert serve.partition(reqs, 1)[0] == sorted(reqs, key=lambda r: r.t_arrive)
+
+
+def test_serve_devices_runs_one_server_per_device():
+    reqs = small_stream(30)
+    rates = {r.rid: 0.02 for r in reqs}
+    made = []
+
+    def make_server(dev):
+        arena = FakeArena(10 ** 9, rates)
+        made.append((dev, arena))
+        return serve.Server(arena, orders=6.0, max_steps=1000, chunk=50, workers=2, keep=lambda rid: True,
+                            mesh_for=lambda r: r)
+
+    res, parts = serve.serve_devices(reqs, make_server, [0, 1])
+    assert sorted(d for d, _ in made) == [0, 1]
+    assert [x.rid for x in res] == sorted(r.rid for r in reqs)
+    for (dev, arena), part in zip(sorted(made, key=lambda m: m[0]), parts):
+        assert sorted(arena.admitted) == sorted(r.rid for r in part)     # each device served its share
+    assert all(x.steps == 300 for x in res)                               # 10**(-0.02 n) <= 1e-6 at n = 300
