@@ -623,35 +623,44 @@ int hcfd_gpu_step(hcfd_solver* s, int nsteps, int time_mode, double dt_or_cfl, h
     if (nsteps < 0 || time_mode < HCFD_FIXED_DT || time_mode > HCFD_LOCAL_CFL || !std::isfinite(dt_or_cfl) || dt_or_cfl < 0)
         return fail(HCFD_EINVAL, "step: bad argument");
     int n = nsteps;
-    if (n >= 2 && !s->prof) {
-        if (s->graph && (s->g_mode != time_mode || s->g_value != dt_or_cfl || s->g_cur != s->cur)) {
-            cudaGraphExecDestroy(s->graph);
-            s->graph = nullptr;
-        }
-        if (!s->graph) {
-            const int cur0 = s->cur;
-            cudaGraph_t g;
-            CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-            for (int k = 0; k < 2 && rc == HCFD_OK; k++)
-                rc = s->fp32() ? launch_step_w<float>(s, time_mode, dt_or_cfl) : launch_step_w<double>(s, time_mode, dt_or_cfl);
-            const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
-            if (rc) return rc;
-            if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("step: capture: ") + cudaGetErrorString(e));
-            const cudaError_t ei = cudaGraphInstantiate(&s->graph, g, 0);
-            cudaGraphDestroy(g);
-            if (ei != cudaSuccess) {
+    while (n > 0) {
+        // pairs of steps without per-kernel events run as the graph; profiled steps run eagerly
+        const bool rec = s->prof && (s->prof_count % s->prof_every == 0 || (s->prof_count + 1) % s->prof_every == 0);
+        if (n >= 2 && !rec) {
+            if (s->graph && (s->g_mode != time_mode || s->g_value != dt_or_cfl || s->g_cur != s->cur)) {
+                cudaGraphExecDestroy(s->graph);
                 s->graph = nullptr;
-                return fail(HCFD_ECUDA, std::string("step: instantiate: ") + cudaGetErrorString(ei));
             }
-            s->g_mode = time_mode;
-            s->g_value = dt_or_cfl;
-            s->g_cur = cur0;   // the capture flipped cur twice: back where it started
+            if (!s->graph) {
+                const int cur0 = s->cur;
+                const bool prof = s->prof;
+                s->prof = false;                 // no events inside the graph
+                cudaGraph_t g;
+                CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+                for (int k = 0; k < 2 && rc == HCFD_OK; k++)
+                    rc = s->fp32() ? launch_step_w<float>(s, time_mode, dt_or_cfl) : launch_step_w<double>(s, time_mode, dt_or_cfl);
+                const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+                s->prof = prof;
+                if (rc) return rc;
+                if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("step: capture: ") + cudaGetErrorString(e));
+                const cudaError_t ei = cudaGraphInstantiate(&s->graph, g, 0);
+                cudaGraphDestroy(g);
+                if (ei != cudaSuccess) {
+                    s->graph = nullptr;
+                    return fail(HCFD_ECUDA, std::string("step: instantiate: ") + cudaGetErrorString(ei));
+                }
+                s->g_mode = time_mode;
+                s->g_value = dt_or_cfl;
+                s->g_cur = cur0;   // the capture flipped cur twice: back where it started
+            }
+            CK(cudaGraphLaunch(s->graph, s->stream));
+            if (s->prof) s->prof_count += 2;
+            n -= 2;
+        } else {
+            rc = s->fp32() ? launch_step_w<float>(s, time_mode, dt_or_cfl) : launch_step_w<double>(s, time_mode, dt_or_cfl);
+            if (rc) return rc;
+            n -= 1;
         }
-        for (; n >= 2; n -= 2) CK(cudaGraphLaunch(s->graph, s->stream));
-    }
-    for (; n > 0; n--) {
-        rc = s->fp32() ? launch_step_w<float>(s, time_mode, dt_or_cfl) : launch_step_w<double>(s, time_mode, dt_or_cfl);
-        if (rc) return rc;
     }
     if (stats) return read_stats(s, stats);
     return HCFD_OK;

@@ -542,17 +542,33 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
     // face phase: one Rusanov flux per face entry (Flux.cpp:19-38).  Each thread takes two
     // entries per round and computes both before storing either, so the two independent
     // FP64 dependency chains (divisions, square roots) interleave.
+    // Threads below nf - NT (per round) have a second entry.  In FP64, whole warps take the
+    // one-entry path when none of their threads has one (the warp that straddles the boundary
+    // takes the two-entry path throughout, its threads without a second entry computing theirs
+    // twice, so that no warp runs both paths one after the other); this saves FP64 work.  In
+    // FP32 every warp takes the two-entry path: the flux is cheap there, and measured on the
+    // B200 the split costs more than it saves.
+    T* sGeoW = reinterpret_cast<T*>(st + L.geo);
     for (int e = threadIdx.x; e < nf; e += 2 * NT) {
-        const int eB = (e + NT < nf) ? e + NT : e;
-        FaceIn<T> A, Bq;
-        A.load(sU, sG, NL, sGeo, sMeta, nf, e);
-        Bq.load(sU, sG, NL, sGeo, sMeta, nf, eB);
-        T FA[4], FB[4];
-        A.flux(s.gma, FA);
-        Bq.flux(s.gma, FB);
-        T* sGeoW = reinterpret_cast<T*>(st + L.geo);
-        A.store(sGeoW, nf, FA);
-        if (eB != e) Bq.store(sGeoW, nf, FB);
+        const int base2 = e - (int) threadIdx.x;                 // first entry of this round
+        const int pairs = min(NT, max(0, nf - base2 - NT));      // threads with a second entry
+        if (sizeof(T) == 4 || (int) (threadIdx.x & ~31u) < pairs) {
+            const int eB = (e + NT < nf) ? e + NT : e;
+            FaceIn<T> A, Bq;
+            A.load(sU, sG, NL, sGeo, sMeta, nf, e);
+            Bq.load(sU, sG, NL, sGeo, sMeta, nf, eB);
+            T FA[4], FB[4];
+            A.flux(s.gma, FA);
+            Bq.flux(s.gma, FB);
+            A.store(sGeoW, nf, FA);
+            if (eB != e) Bq.store(sGeoW, nf, FB);
+        } else {
+            FaceIn<T> A;
+            A.load(sU, sG, NL, sGeo, sMeta, nf, e);
+            T FA[4];
+            A.flux(s.gma, FA);
+            A.store(sGeoW, nf, FA);
+        }
     }
     compute_sync(NT);
     // cell phase: slots in increasing face order, update, ghost refresh
