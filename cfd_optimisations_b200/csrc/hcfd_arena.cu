@@ -80,52 +80,61 @@ struct Inst {
     long long admitted_step = 0;
 };
 
-// Per active instance: its slot and its tile range in the active list.
-__global__ void __launch_bounds__(512) arena_finalize_kernel(int nact, const int4* __restrict__ act,
-                                                             const double* __restrict__ tile_r2,
-                                                             const int* __restrict__ tile_bad,
-                                                             const double* __restrict__ inst_dt,
-                                                             unsigned long long* inst_dtmin, hcfd::StepStats* stats,
-                                                             int time_mode, int par) {
-    __shared__ double sx[16];
-    __shared__ int sb[16];
-    const int i = blockIdx.x;
+// Residual of each instance in two stages, both in an order fixed relative to the
+// instance's first tile, so that it does not depend on where the instance sits in the arena.
+// Stage 1: a block per chunk of kChunk per-warp partials of one instance (thread k takes
+// partials k, k + 256, ..., then the threads in a fixed tree).
+constexpr int kChunk = 8192;
+__global__ void __launch_bounds__(256) arena_chunk_kernel(const int4* __restrict__ chunks,
+                                                          const double* __restrict__ tile_r2,
+                                                          const int* __restrict__ tile_bad, double* __restrict__ chunk_r2,
+                                                          int* __restrict__ chunk_bad) {
+    __shared__ double sx[8];
+    __shared__ int sb[8];
+    const int4 c = chunks[blockIdx.x];               // {act index, first partial, end, -}
+    double x0 = 0.0, x1 = 0.0;
+    int b = 0;
+    int j = c.y + (int) threadIdx.x;
+    for (; j + 256 < c.z; j += 512) {
+        x0 += tile_r2[j];
+        x1 += tile_r2[j + 256];
+        b |= tile_bad[j] | tile_bad[j + 256];
+    }
+    for (; j < c.z; j += 256) { x0 += tile_r2[j]; b |= tile_bad[j]; }
+    const double x = hcfd::warp_sum(x0 + x1);
+    b = __any_sync(0xffffffffu, b);
+    if ((threadIdx.x & 31) == 0) { sx[threadIdx.x >> 5] = x; sb[threadIdx.x >> 5] = b; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        int bb = 0;
+        for (int w = 0; w < 8; w++) { t += sx[w]; bb |= sb[w]; }
+        chunk_r2[blockIdx.x] = t;
+        chunk_bad[blockIdx.x] = bb;
+    }
+}
+
+// Stage 2, per active instance {slot, first tile, end tile, first chunk}: its chunks in
+// order, then the step statistics and dt bookkeeping.
+__global__ void arena_finalize_kernel(int nact, int nchunks, const int4* __restrict__ act,
+                                      const double* __restrict__ chunk_r2, const int* __restrict__ chunk_bad,
+                                      const double* __restrict__ inst_dt, unsigned long long* inst_dtmin,
+                                      hcfd::StepStats* stats, int time_mode, int par) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nact) return;
     const int4 d = act[i];
-    const int slot = d.x, t0 = d.y, t1 = d.z;
-    // The instance's tiles are summed in an order fixed relative to its first tile (thread
-    // k takes tiles k, k + 512, ... in four interleaved chains, then the threads in a fixed
-    // tree), so the residual does not depend on where the instance sits in the arena.
-    const int k = threadIdx.x, n = t1 - t0;
-    double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+    const int slot = d.x, c0 = d.w, c1 = i + 1 < nact ? act[i + 1].w : nchunks;
+    double x = 0.0;
     int b = 0;
-    int j = k;
-    for (; j + 3 * 512 < n; j += 4 * 512) {
-        x0 += tile_r2[t0 + j];
-        x1 += tile_r2[t0 + j + 512];
-        x2 += tile_r2[t0 + j + 1024];
-        x3 += tile_r2[t0 + j + 1536];
-        b |= tile_bad[t0 + j] | tile_bad[t0 + j + 512] | tile_bad[t0 + j + 1024] | tile_bad[t0 + j + 1536];
-    }
-    for (; j < n; j += 512) { x0 += tile_r2[t0 + j]; b |= tile_bad[t0 + j]; }
-    double x = hcfd::warp_sum((x0 + x1) + (x2 + x3));
-    b = __any_sync(0xffffffffu, b);
-    const int lane = k & 31, wid = k >> 5;
-    if (lane == 0) { sx[wid] = x; sb[wid] = b; }
-    __syncthreads();
-    if (k == 0) {
-        x = 0.0;
-        b = 0;
-        for (int w = 0; w < (int) (blockDim.x >> 5); w++) { x += sx[w]; b |= sb[w]; }
-        hcfd::StepStats* st = stats + slot;
-        st->res2_last = x;
-        if (st->steps == 0) st->res2_first = x;
-        st->steps += 1;
-        const double v = inst_dt[slot];
-        st->dt_last = time_mode == hcfd::TM_FIXED ? v : v * __longlong_as_double((long long) inst_dtmin[2 * slot + par]);
-        if (b || !(x == x) || x > 1.7e308) st->nonfinite = 1;
-        inst_dtmin[2 * slot + (1 - par)] = 0x7FF0000000000000ULL;
-    }
+    for (int c = c0; c < c1; c++) { x += chunk_r2[c]; b |= chunk_bad[c]; }
+    hcfd::StepStats* st = stats + slot;
+    st->res2_last = x;
+    if (st->steps == 0) st->res2_first = x;
+    st->steps += 1;
+    const double v = inst_dt[slot];
+    st->dt_last = time_mode == hcfd::TM_FIXED ? v : v * __longlong_as_double((long long) inst_dtmin[2 * slot + par]);
+    if (b || !(x == x) || x > 1.7e308) st->nonfinite = 1;
+    inst_dtmin[2 * slot + (1 - par)] = 0x7FF0000000000000ULL;
 }
 
 template <class T>
@@ -203,6 +212,7 @@ struct hcfd_arena {
     // host copies of the last active-list upload and the event after which they may change
     std::vector<int> tl_host;
     std::vector<int4> act_host;
+    std::vector<int4> chunk_host;
     cudaEvent_t list_ev = nullptr;
     bool list_pending = false;
     size_t Ccap = 0, Ecap = 0, HLcap = 0;
@@ -223,6 +233,11 @@ struct hcfd_arena {
     hcfd::StepStats* stats = nullptr;
     int4* tiles = nullptr;
     int4* act = nullptr;
+    int4* chunks = nullptr;                 // residual chunks of the active instances
+    double* chunk_r2 = nullptr;
+    int* chunk_bad = nullptr;
+    size_t chunks_cap = 0;
+    int nchunks = 0;
     double* tile_r2 = nullptr;
     int* tile_bad = nullptr;
     unsigned int* err = nullptr;
@@ -311,8 +326,10 @@ int enqueue_step(hcfd_arena* A, int cur, int par) {
     constexpr bool COMP = std::is_same<T, float>::value;
     hcfd::tile_pass1_kernel<T, W, true><<<A->grid1, A->B + 32, A->smem1, A->stream>>>(a);
     hcfd::tile_pass2_kernel<T, W, COMP, true><<<A->grid2, A->B + 32, A->smem2, A->stream>>>(a);
-    arena_finalize_kernel<<<A->nact, 512, 0, A->stream>>>(A->nact, A->act, A->tile_r2, A->tile_bad, A->inst_dt,
-                                                         A->inst_dtmin, A->stats, A->time_mode, par);
+    arena_chunk_kernel<<<A->nchunks, 256, 0, A->stream>>>(A->chunks, A->tile_r2, A->tile_bad, A->chunk_r2, A->chunk_bad);
+    arena_finalize_kernel<<<(A->nact + 127) / 128, 128, 0, A->stream>>>(A->nact, A->nchunks, A->act, A->chunk_r2,
+                                                                       A->chunk_bad, A->inst_dt, A->inst_dtmin, A->stats,
+                                                                       A->time_mode, par);
     CK(cudaGetLastError());
     return HCFD_OK;
 }
@@ -367,6 +384,9 @@ int rebuild_active(hcfd_arena* A) {
     if (A->list_pending) CK(cudaEventSynchronize(A->list_ev));
     std::vector<int>& tl = A->tl_host;
     std::vector<int4>& act = A->act_host;
+    std::vector<int4>& chk = A->chunk_host;
+    chk.clear();
+    const int nw = A->B / 32;
     tl.clear();
     act.clear();
     int hmax = 0, fmax = 4;
@@ -377,7 +397,10 @@ int rebuild_active(hcfd_arena* A) {
         hmax = std::max(hmax, I.Hmax);
         fmax = std::max(fmax, I.Fmax);
         tl.insert(tl.end(), I.tiles.begin(), I.tiles.end());
-        act.push_back(make_int4((int) k, t0, (int) (tl.size() / 8), 0));
+        const int t1 = (int) (tl.size() / 8);
+        act.push_back(make_int4((int) k, t0, t1, (int) chk.size()));
+        for (int p = t0 * nw; p < t1 * nw; p += kChunk)
+            chk.push_back(make_int4((int) act.size() - 1, p, std::min(p + kChunk, t1 * nw), 0));
     }
     A->nact_tiles = (int) (tl.size() / 8);
     A->nact = (int) act.size();
@@ -385,6 +408,9 @@ int rebuild_active(hcfd_arena* A) {
     // stream-ordered after the steps already enqueued, before the next ones
     if (!tl.empty()) CK(cudaMemcpyAsync(A->tiles, tl.data(), sizeof(int) * tl.size(), cudaMemcpyHostToDevice, A->stream));
     if (!act.empty()) CK(cudaMemcpyAsync(A->act, act.data(), sizeof(int4) * act.size(), cudaMemcpyHostToDevice, A->stream));
+    if (chk.size() > A->chunks_cap) return fail(HCFD_EINVAL, "arena: residual chunk capacity exceeded");
+    A->nchunks = (int) chk.size();
+    if (!chk.empty()) CK(cudaMemcpyAsync(A->chunks, chk.data(), sizeof(int4) * chk.size(), cudaMemcpyHostToDevice, A->stream));
     CK(cudaEventRecord(A->list_ev, A->stream));
     A->list_pending = true;
     free_graph(A);
@@ -415,7 +441,8 @@ void arena_free(hcfd_arena* A) {
     if (A->list_ev) cudaEventDestroy(A->list_ev);
     if (A->astream) cudaStreamDestroy(A->astream);
     void* p[] = {A->U[0], A->U[1], A->phiG, A->phiF, A->iv, A->cslot, A->tgeo, A->tmeta, A->halo, A->inst_dt, A->inst_dtmin,
-                 A->inst_bc, A->stats, A->tiles, A->act, A->tile_r2, A->tile_bad, A->err};
+                 A->inst_bc, A->stats, A->tiles, A->act, A->tile_r2, A->tile_bad, A->err, A->chunks, A->chunk_r2,
+                 A->chunk_bad};
     for (void* q : p) if (q) cudaFree(q);
     if (A->stream) cudaStreamDestroy(A->stream);
 }
@@ -469,6 +496,7 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
     A->Ecap = (size_t) (1.75 * C) / 4 * 4;
     A->HLcap = (size_t) (0.6 * C);
     A->tiles_cap = C / A->B;
+    A->chunks_cap = A->tiles_cap * (A->B / 32) / kChunk + p.max_instances + 1;
     A->fc.init(C / A->B);
     A->fe.init(A->Ecap / 4);
     A->fh.init(A->HLcap);
@@ -488,7 +516,9 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
         (rc = dalloc(&h->inst_dt, p.max_instances)) || (rc = dalloc(&h->inst_dtmin, 2 * (size_t) p.max_instances)) ||
         (rc = dalloc(&h->inst_bc, p.max_instances)) || (rc = dalloc(&h->stats, p.max_instances)) ||
         (rc = dalloc(&h->tiles, 2 * h->tiles_cap)) || (rc = dalloc(&h->act, p.max_instances)) ||
-        (rc = dalloc(&h->tile_r2, h->tiles_cap)) || (rc = dalloc(&h->tile_bad, h->tiles_cap)) || (rc = dalloc(&h->err, 1)))
+        (rc = dalloc(&h->tile_r2, h->tiles_cap * (h->B / 32))) || (rc = dalloc(&h->tile_bad, h->tiles_cap * (h->B / 32))) ||
+        (rc = dalloc(&h->err, 1)) || (rc = dalloc(&h->chunks, h->chunks_cap)) ||
+        (rc = dalloc(&h->chunk_r2, h->chunks_cap)) || (rc = dalloc(&h->chunk_bad, h->chunks_cap)))
         return bail(rc);
     cudaError_t ce = cudaMemsetAsync(h->err, 0, sizeof(unsigned int), h->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->U[0], 0, 4 * ts * C, h->stream);

@@ -36,8 +36,8 @@ struct TileArgs {
     unsigned long long* inst_dtmin;        // per instance, two parity slots (double bits)
     const BCTable* __restrict__ inst_bc;   // per instance
     const StepStats* inst_stats;           // per instance (step counts for limiter freezing)
-    double* tile_r2;                       // per active tile: sum of R_rho^2 of its cells
-    int* tile_bad;                         // per active tile: a NaN/Inf appeared
+    double* tile_r2;                       // per active tile and compute warp (t * B/32 + warp): sum of R_rho^2
+    int* tile_bad;                         // same layout: a NaN/Inf appeared
     int par;                               // which dtmin slot this step uses
 };
 
@@ -61,7 +61,7 @@ __device__ __forceinline__ void tile_info(const TileArgs<T>& a, int t, int& base
 // warps start a tile without dependent global loads: its descriptor, and for its instance
 // the step count (limiter freezing), the dt or CFL number and the dt minimum of this step.
 struct StageInfo {
-    int base, nb, f0, nf, h0, nh, inst, pad;
+    int base, nb, f0, nf, h0, nh, inst, next_inst;   // next_inst (pass 1, arena): of this CTA's next tile, -1 at the end
     double dt_or_cfl;
     double dtmin;
     long long steps;
@@ -201,10 +201,29 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
     unsigned iter = 0;
     for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {
         const int buf = iter & 1;
-        if (iter >= 2) mbar_wait(empty + buf, ((iter >> 1) - 1) & 1, a.err);
-        unsigned char* st = smem + kHeader + buf * L.stage;
+        // the tile's descriptor and its instance's scalars are loaded before the wait for the
+        // stage, so that their latency hides behind it (none of them changes during the kernel
+        // in a way the kernel reads: dt minima and step counts come from earlier kernels)
         int base, nb, f0, nf, h0, nh, inst;
         tile_info<ARENA>(a, t, base, nb, f0, nf, h0, nh, inst);
+        double v_dt = 0.0, v_dtmin = 0.0;
+        long long v_steps = 0;
+        int v_next = -1;
+        if (lane == 0) {
+            if constexpr (ARENA) {
+                v_dt = __ldg(a.inst_dt + inst);
+                v_dtmin = __longlong_as_double((long long) a.inst_dtmin[2 * inst + a.par]);
+                v_steps = a.inst_stats[inst].steps;
+                const int tn = t + (int) gridDim.x;
+                if (!PASS2 && tn < a.ntiles) v_next = __ldg(&a.tiles[2 * tn].w);
+            } else {
+                v_dt = a.s.dt_or_cfl;
+                v_dtmin = __longlong_as_double((long long) *a.s.dtmin);
+                v_steps = a.s.stats->steps;
+            }
+        }
+        if (iter >= 2) mbar_wait(empty + buf, ((iter >> 1) - 1) & 1, a.err);
+        unsigned char* st = smem + kHeader + buf * L.stage;
         Cell4<T>* sU = reinterpret_cast<Cell4<T>*>(st + L.u);
         Grad8<T>* sG = reinterpret_cast<Grad8<T>*>(st + L.g);
         if (lane == 0) {
@@ -215,15 +234,10 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
             // arrive below
             StageInfo* si = reinterpret_cast<StageInfo*>(smem + 64) + buf;
             si->base = base; si->nb = nb; si->f0 = f0; si->nf = nf; si->h0 = h0; si->nh = nh; si->inst = inst;
-            if constexpr (ARENA) {
-                si->dt_or_cfl = __ldg(a.inst_dt + inst);
-                si->dtmin = __longlong_as_double((long long) a.inst_dtmin[2 * inst + a.par]);
-                si->steps = a.inst_stats[inst].steps;
-            } else {
-                si->dt_or_cfl = a.s.dt_or_cfl;
-                si->dtmin = __longlong_as_double((long long) *a.s.dtmin);
-                si->steps = a.s.stats->steps;
-            }
+            si->next_inst = v_next;                  // pass 1 in arena mode only
+            si->dt_or_cfl = v_dt;
+            si->dtmin = v_dtmin;
+            si->steps = v_steps;
             mbar_arrive_expect_tx(full + buf, bu + bg + bf + bm + bs + bi);
             // one bulk copy per 16-byte chunk plane of the tile's cell range
 #pragma unroll
@@ -500,8 +514,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
         // next tile belongs to another instance, so a large instance sees a few atomics per
         // CTA rather than one per warp and tile on a single address
         if (s.time_mode != TM_FIXED) {
-            const int tn = t + (int) gridDim.x;
-            if (tn >= a.ntiles || __ldg(&a.tiles[2 * tn].w) != inst) {
+            if (si.next_inst != inst) {
                 const double m = warp_min(dtc);
                 if ((threadIdx.x & 31) == 0 && m < 1e300)
                     atomicMin(a.inst_dtmin + 2 * inst + a.par, (unsigned long long) __double_as_longlong(m));
@@ -532,8 +545,6 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
     double dt_used = 0.0;
     double r2 = 0.0;
     int bad = 0;
-    __shared__ double s_wr2[8];
-    __shared__ int s_wbad[8];
     HCFD_TILE_LOOP_BEGIN(true, ARENA)
     const T cfl_or_dt = T(si.dt_or_cfl);
     dt_used = (s.time_mode == TM_FIXED) ? si.dt_or_cfl : si.dt_or_cfl * si.dtmin;
@@ -639,22 +650,17 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
         }
     }
     if constexpr (ARENA) {
-        // per-tile residual: warp sums, then the warps in order (deterministic)
+        // per-tile residual: one partial per warp (fixed order, no barrier); the finalize
+        // kernel sums an instance's partials in order
         const double w = warp_sum(r2);
         const int wb = __any_sync(0xffffffffu, bad);
-        if ((threadIdx.x & 31) == 0) { s_wr2[threadIdx.x >> 5] = w; s_wbad[threadIdx.x >> 5] = wb; }
+        if ((threadIdx.x & 31) == 0) {
+            const int k = t * (NT >> 5) + (int) (threadIdx.x >> 5);
+            a.tile_r2[k] = w;
+            a.tile_bad[k] = wb;
+        }
         r2 = 0.0;
         bad = 0;
-    }
-    if constexpr (ARENA) {
-        compute_sync(NT);   // every warp's tile partial is in s_wr2 / s_wbad
-        if (threadIdx.x == 0) {
-            double tot = 0.0;
-            int b = 0;
-            for (int k = 0; k < NT / 32; k++) { tot += s_wr2[k]; b |= s_wbad[k]; }
-            a.tile_r2[t] = tot;
-            a.tile_bad[t] = b;
-        }
     }
     HCFD_TILE_LOOP_END
     if constexpr (!ARENA) finish_step(s, r2, bad, dt_used);
