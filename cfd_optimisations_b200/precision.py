@@ -15,6 +15,8 @@ against FP64 (relative L-inf and L2 of each conserved variable, and the L-inf an
 the wall pressure coefficient on the lower wall, the ramp).  A third run, FP64 from an initial
 density one rounding step larger, gives the same errors for a perturbation the size of one
 rounding: the floor that no precision can go below while the limiter keeps switching.
+With --track N the three solves instead step side by side to --max-steps, their errors
+against FP64 recorded every N steps, to show how long each stays within 1e-5.
 """
 from __future__ import annotations
 
@@ -84,6 +86,42 @@ def errors(a: dict, b: dict) -> dict:
                 cp_l2=float(np.sqrt((dcp ** 2).mean())), cp_range=float(b["cp"].max() - b["cp"].min()))
 
 
+def _rel_linf(Ua: np.ndarray, Ub: np.ndarray) -> float:
+    return float((np.abs(Ua - Ub).max(axis=1) / np.abs(Ub).max(axis=1)).max())
+
+
+def track(mesh: Mesh, mach: float, cfl: float, steps: int, every: int, mode: int = LOCAL_CFL,
+          limiter: int = LIMITER_VENKAT, K: float = 5.0, freeze: int = 0, bound: float = 1e-5) -> dict:
+    """Steps the FP64 solve, the FP32 solve and the FP64 solve from an initial density one
+    rounding step larger side by side and records, every `every` steps, the relative L-inf
+    error (max over the conserved variables) of the last two against the first; returns the
+    history and the last recorded step at which each error was still within `bound`."""
+    bcmap, qbc, q = wedge_case(mach)
+    runs = {}
+    for name, prec, scale in (("fp64", FP64, 1.0), ("fp32", FP32, 1.0), ("fp64_perturbed", FP64, 1.0 + 2.0 ** -52)):
+        s = Solver(mesh, limiter=limiter, venkat_K=K, precision=prec, freeze_limiter_after=freeze)
+        s.gather_bcs(bcmap, qbc)
+        qi = list(q)
+        qi[0] *= scale
+        s.initialise(qi)
+        runs[name] = s
+    hist, within = [], {"fp32": 0, "fp64_perturbed": 0}
+    done = 0
+    while done < steps:
+        n = min(every, steps - done)
+        for s in runs.values():
+            s.step(n, mode, cfl)
+        done += n
+        U64 = runs["fp64"].U()
+        row = dict(step=done, res_l2=runs["fp64"].stats()["res_l2"])
+        for k in within:
+            row[k] = _rel_linf(runs[k].U(), U64)
+            if row[k] <= bound and within[k] == done - n:
+                within[k] = done
+        hist.append(row)
+    return dict(bound=bound, steps_within_bound=within, history=hist)
+
+
 def study(nx=1025, ny=513, mach=3.0, theta=20.0, cfl=0.8, orders=8.0, max_steps=50000, seed=1234,
           mode=LOCAL_CFL, limiter=LIMITER_VENKAT, K=5.0, freeze=0) -> dict:
     mesh = Mesh.wedge(nx, ny, theta_deg=theta, seed=seed, numbering=NUMBER_RANDOM)
@@ -122,10 +160,23 @@ def main():
     ap.add_argument("--K", type=float, default=5.0)
     ap.add_argument("--freeze", type=int, default=0,
                     help="freeze the limiter after this many steps (0: never)")
+    ap.add_argument("--track", type=int, default=0,
+                    help="instead of the convergence runs: step all three solves to --max-steps and "
+                         "record their errors every this many steps")
     a = ap.parse_args()
+    mode = GLOBAL_CFL if a.global_dt else LOCAL_CFL
+    limiter = LIMITER_BJ if a.bj else LIMITER_VENKAT
+    if a.track:
+        mesh = Mesh.wedge(a.nx, a.ny, theta_deg=a.theta, seed=1234, numbering=NUMBER_RANDOM)
+        out = track(mesh, a.mach, a.cfl, a.max_steps, a.track, mode=mode, limiter=limiter, K=a.K, freeze=a.freeze)
+        out["workload"] = dict(nx=a.nx, ny=a.ny, mach=a.mach, theta_deg=a.theta, cfl=a.cfl,
+                               time_mode="local" if mode == LOCAL_CFL else "global",
+                               limiter="bj" if a.bj else "venkatakrishnan", K=a.K, steps=a.max_steps,
+                               freeze_limiter_after=a.freeze)
+        print(json.dumps(out))
+        return
     print(json.dumps(study(a.nx, a.ny, a.mach, a.theta, a.cfl, a.orders, a.max_steps,
-                           mode=GLOBAL_CFL if a.global_dt else LOCAL_CFL,
-                           limiter=LIMITER_BJ if a.bj else LIMITER_VENKAT, K=a.K, freeze=a.freeze)))
+                           mode=mode, limiter=limiter, K=a.K, freeze=a.freeze)))
 
 
 if __name__ == "__main__":
