@@ -136,3 +136,25 @@ def test_export_vtu_round_trip(tmp_path):
     out = meshio.batch_export(str(tmp_path / "r.hmsh"), str(tmp_path / "s_%d.hsln"), str(tmp_path / "o_%d.vtu"))
     assert out == [str(tmp_path / "o_3.vtu")]
     assert meshio.check_cell(str(tmp_path / "r.hmsh"), 0)["cell"] == 0
+
+
+@pytest.mark.skipif(not O.RefSolver.available(), reason="reference not compiled into oracle/_ref")
+def test_oracle_matches_reference_on_an_imported_mixed_mesh(tmp_path):
+    """The reference's Base solver (compiled unchanged) reads the imported quadrangle/triangle
+    mesh with its own reader and steps it; the oracle stays bit-identical to it, so the GPU's
+    parity against the oracle on this mesh is parity against the reference."""
+    write_msh(tmp_path / "r.msh", nx=41, ny=21)
+    meshio.import_msh(str(tmp_path / "r.msh"), str(tmp_path / "r.hmsh"))
+    path = str(tmp_path / "r.hmsh")
+    bcmap = [O.SYMMETRY, O.SYMMETRY, O.SUPOUTLET, O.SYMMETRY, O.SUPINLET]
+    q = np.array([1.4, 2.2, 0.35, 1.0])
+    qbc = np.tile(q, (4, 1))
+    o = O.Oracle(O.read_hmsh(path))
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    U0 = o.U()
+    dts = [o.step(O.GLOBAL_CFL, 0.5)[0] for _ in range(50)]
+    r = O.RefSolver(path, np.array(bcmap), qbc, q)
+    r.steps(50, np.array(dts))
+    assert np.max(np.abs(o.U() - U0)) > 1e-2          # the walls have turned the flow
+    assert np.array_equal(o.U(), r.U())
