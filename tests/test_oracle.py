@@ -68,6 +68,22 @@ def test_reference_build_reproduces_goldens(golden):
 
 
 @pytest.mark.skipif(not O.RefSolver.available(), reason="reference not compiled into oracle/_ref")
+def test_timed_reference_layout_matches_base(golden):
+    """The layout the CPU baseline times (VEC, 4-wide AVX2) computes the same solution as the
+    Base layout: within 1e-12 after one step and 1e-9 after the 1000 steps of Base_1.hsln."""
+    bcmap, qbc, q = wedge_case_ref()
+    path = os.path.join(golden, "wedge.hmsh")
+    _, b1 = O.read_hsln(os.path.join(golden, "Base_1.hsln"))
+    base = O.RefSolver(path, bcmap, qbc, q, layout="Base")
+    vec = O.RefSolver(path, bcmap, qbc, q, layout="VEC")
+    base.steps(1, 1e-3)
+    vec.steps(1, 1e-3)
+    assert np.all(O.rel_linf(vec.U(), base.U()) <= 1e-12)
+    vec.steps(999, 1e-3)
+    assert np.all(O.rel_linf(vec.Q(), b1) <= 1e-9)
+
+
+@pytest.mark.skipif(not O.RefSolver.available(), reason="reference not compiled into oracle/_ref")
 @pytest.mark.parametrize("numbering", [H.NUMBER_NATURAL, H.NUMBER_RANDOM, H.NUMBER_RCM, H.NUMBER_MORTON])
 def test_oracle_matches_reference_on_generated_meshes(tmp_path, numbering):
     m = H.Mesh.wedge(41, 21, seed=3, numbering=numbering)
