@@ -2,10 +2,12 @@
 class.
 
 Two tunings:
-  - a single-mesh solver (Solver): the tiled kernels with 64, 128 or 256 cells per tile
-    (one compute thread per cell, or 128 threads over 256 cells — two cells per thread)
-    against the per-cell kernels with 128 or 256 threads per block (no tile staging: the
-    other fusion split), timed on one wedge of the size class;
+  - a single-mesh solver (Solver): the tiled kernels with 64, 128 or 256 cells per tile for
+    both passes (one compute thread per cell, or 128 threads over 256 cells — two cells per
+    thread), with separate pass-1 / pass-2 tilings (the library's default, 224 / 192 cells in
+    FP64 and 256 / 128 in FP32, and 256 / 128), against the per-cell kernels with 128 or
+    256 threads per block (no tile staging: the other fusion split), timed on one wedge of
+    the size class;
   - an arena (Arena): its tile size (64, 128 or 256 cells, one thread per cell), timed on
     an arena holding copies of a wedge of the size class, about 2 million cells in all, so
     that the timing is that of a full device and not of one launch-bound instance.
@@ -24,13 +26,16 @@ from . import (FP64, GLOBAL_CFL, KERNEL_CELL, KERNEL_TILED, LIMITER_BJ, NUMBER_R
                wedge_case)
 
 SOLVER_SHAPES = (
-    dict(kernel=KERNEL_TILED, tile=64, block=64),
-    dict(kernel=KERNEL_TILED, tile=128, block=128),
-    dict(kernel=KERNEL_TILED, tile=256, block=256),
-    dict(kernel=KERNEL_TILED, tile=256, block=128),
-    dict(kernel=KERNEL_CELL, tile=0, block=128),
-    dict(kernel=KERNEL_CELL, tile=0, block=256),
+    dict(kernel=KERNEL_TILED, tile=0, tile2=0, block=0),          # the library's default split
+    dict(kernel=KERNEL_TILED, tile=256, tile2=128, block=0),
+    dict(kernel=KERNEL_TILED, tile=64, tile2=0, block=64),
+    dict(kernel=KERNEL_TILED, tile=128, tile2=0, block=128),
+    dict(kernel=KERNEL_TILED, tile=256, tile2=0, block=256),
+    dict(kernel=KERNEL_TILED, tile=256, tile2=0, block=128),
+    dict(kernel=KERNEL_CELL, tile=0, tile2=0, block=128),
+    dict(kernel=KERNEL_CELL, tile=0, tile2=0, block=256),
 )
+DEFAULT_SHAPE = SOLVER_SHAPES[0]
 ARENA_TILES = (64, 128, 256)
 
 
@@ -122,18 +127,19 @@ def tune_arena(cls: int, precision: int, limiter: int = LIMITER_BJ, steps: int =
 
 
 def best_solver_shape(ncells: int, precision: int = FP64, limiter: int = LIMITER_BJ, tune: bool = True) -> dict:
-    """The cached winner for a single mesh of this size ({kernel, tile, block}); tuned and
-    cached when missing and `tune` is true, else the default shape."""
+    """The cached winner for a single mesh of this size ({kernel, tile, tile2, block}, the
+    Solver keywords); tuned and cached when missing and `tune` is true, else the library's
+    default shape."""
     cls = size_class(ncells)
     key = _key("solver", cls, precision, limiter)
     d = _load()
-    if key not in d:
+    if key not in d or "tile2" not in d[key]["best"]:
         if not tune:
-            return dict(kernel=KERNEL_TILED, tile=128, block=128)
+            return dict(DEFAULT_SHAPE)
         d[key] = tune_solver(cls, precision, limiter)
         _store(d)
     b = d[key]["best"]
-    return dict(kernel=b["kernel"], tile=b["tile"], block=b["block"])
+    return dict(kernel=b["kernel"], tile=b["tile"], tile2=b["tile2"], block=b["block"])
 
 
 def best_arena_tile(ncells: int, precision: int, limiter: int = LIMITER_BJ, tune: bool = True) -> int:
