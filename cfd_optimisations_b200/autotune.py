@@ -13,6 +13,8 @@ Two tunings:
     that the timing is that of a full device and not of one launch-bound instance.
 A size class is round(log2(real cells)), clamped to [10, 24].  The winners are stored in a
 JSON cache ($HCFD_AUTOTUNE_CACHE, default ~/.cache/hcfd_b200/autotune.json).
+
+    python -m cfd_optimisations_b200.autotune --cells N [--fp32] [--arena]
 """
 from __future__ import annotations
 
@@ -153,3 +155,20 @@ def best_arena_tile(ncells: int, precision: int, limiter: int = LIMITER_BJ, tune
         d[key] = tune_arena(cls, precision, limiter)
         _store(d)
     return int(d[key]["best"]["tile"])
+
+
+def main():
+    import argparse
+    from . import FP32
+    ap = argparse.ArgumentParser(description="tune (or read from the cache) the launch shape for a mesh size")
+    ap.add_argument("--cells", type=int, required=True, help="real cells of the mesh (or of a typical instance)")
+    ap.add_argument("--fp32", action="store_true")
+    ap.add_argument("--arena", action="store_true", help="the arena tile size instead of the single-mesh shape")
+    a = ap.parse_args()
+    prec = FP32 if a.fp32 else FP64
+    out = (dict(tile=best_arena_tile(a.cells, prec)) if a.arena else best_solver_shape(a.cells, prec))
+    print(json.dumps(dict(size_class=size_class(a.cells), cache=cache_path(), **out)))
+
+
+if __name__ == "__main__":
+    main()
