@@ -90,12 +90,18 @@ def _rel_linf(Ua: np.ndarray, Ub: np.ndarray) -> float:
     return float((np.abs(Ua - Ub).max(axis=1) / np.abs(Ub).max(axis=1)).max())
 
 
+def _rel_l2(Ua: np.ndarray, Ub: np.ndarray) -> float:
+    return float((np.sqrt(((Ua - Ub) ** 2).mean(axis=1)) / np.sqrt((Ub ** 2).mean(axis=1))).max())
+
+
 def track(mesh: Mesh, mach: float, cfl: float, steps: int, every: int, mode: int = LOCAL_CFL,
           limiter: int = LIMITER_VENKAT, K: float = 5.0, freeze: int = 0, bound: float = 1e-5) -> dict:
     """Steps the FP64 solve, the FP32 solve and the FP64 solve from an initial density one
-    rounding step larger side by side and records, every `every` steps, the relative L-inf
-    error (max over the conserved variables) of the last two against the first; returns the
-    history and the last recorded step at which each error was still within `bound`."""
+    rounding step larger side by side.  Every `every` steps it records the relative L-inf and
+    L2 errors (each the max over the conserved variables) of the last two against the first.
+    Returns the history and the last recorded step at which each L-inf error was still within
+    `bound`.  A solve that produces a NaN or Inf ends the tracking; `diverged` names it and the
+    step by which it did (the end of the interval it failed in)."""
     bcmap, qbc, q = wedge_case(mach)
     runs = {}
     for name, prec, scale in (("fp64", FP64, 1.0), ("fp32", FP32, 1.0), ("fp64_perturbed", FP64, 1.0 + 2.0 ** -52)):
@@ -106,20 +112,30 @@ def track(mesh: Mesh, mach: float, cfl: float, steps: int, every: int, mode: int
         s.initialise(qi)
         runs[name] = s
     hist, within = [], {"fp32": 0, "fp64_perturbed": 0}
-    done = 0
+    done, diverged = 0, None
     while done < steps:
         n = min(every, steps - done)
-        for s in runs.values():
-            s.step(n, mode, cfl)
+        for name, s in runs.items():
+            try:
+                s.step(n, mode, cfl)
+            except HcfdError as e:
+                if e.code != ENONFINITE:
+                    raise
+                diverged = dict(solve=name, by_step=done + n)
+                break
+        if diverged is not None:
+            break
         done += n
         U64 = runs["fp64"].U()
         row = dict(step=done, res_l2=runs["fp64"].stats()["res_l2"])
         for k in within:
-            row[k] = _rel_linf(runs[k].U(), U64)
+            Uk = runs[k].U()
+            row[k] = _rel_linf(Uk, U64)
+            row[k + "_l2"] = _rel_l2(Uk, U64)
             if row[k] <= bound and within[k] == done - n:
                 within[k] = done
         hist.append(row)
-    return dict(bound=bound, steps_within_bound=within, history=hist)
+    return dict(bound=bound, steps_within_bound=within, diverged=diverged, history=hist)
 
 
 def study(nx=1025, ny=513, mach=3.0, theta=20.0, cfl=0.8, orders=8.0, max_steps=50000, seed=1234,

@@ -1,0 +1,55 @@
+"""The precision study's lockstep tracking (precision.track) on the CPU, with stand-in solvers
+whose states drift from the FP64 one at set rates: the bookkeeping of the errors, of the last
+step within the bound, and of a solve that produces a NaN or Inf."""
+import numpy as np
+import pytest
+
+from cfd_optimisations_b200 import precision as P
+from cfd_optimisations_b200.native import ENONFINITE, HcfdError
+
+
+def fake_solver(drift, fail_after=None):
+    """A stand-in for Solver: state 1 + drift(step) per precision, NaN/Inf error after
+    `fail_after` steps of one precision."""
+    class S:
+        def __init__(self, mesh, precision, freeze_limiter_after=0, **kw):
+            self.prec, self.n, self.scale = precision, 0, 1.0
+
+        def gather_bcs(self, bcmap, qbc):
+            pass
+
+        def initialise(self, q):
+            self.scale = q[0] / 1.4
+
+        def step(self, n, mode, cfl):
+            self.n += n
+            if fail_after is not None and self.prec == P.FP32 and self.n > fail_after:
+                raise HcfdError(ENONFINITE, "a step produced a NaN or Inf")
+
+        def stats(self):
+            return dict(res_l2=1.0 / self.n)
+
+        def U(self):
+            e = drift(self.n) if self.prec == P.FP32 else (self.scale - 1.0) * 1e6 * self.n
+            return np.full((4, 8), 1.0 + e)
+    return S
+
+
+def test_track_records_errors_and_the_horizon(monkeypatch):
+    monkeypatch.setattr(P, "Solver", fake_solver(lambda n: 1e-7 * 2.0 ** (n / 10)))
+    out = P.track(None, 2.5, 0.5, steps=100, every=10)
+    steps = [r["step"] for r in out["history"]]
+    assert steps == list(range(10, 101, 10)) and out["diverged"] is None
+    # FP32 drift 1e-7 * 2**(n/10): within 1e-5 while 2**(n/10) <= 100, i.e. up to step 60
+    assert out["steps_within_bound"]["fp32"] == 60
+    r = out["history"][0]
+    assert r["fp32"] == pytest.approx(2e-7, rel=1e-6) and r["fp32_l2"] == pytest.approx(2e-7, rel=1e-6)
+    # the perturbed FP64 solve: (2**-52 * 1e6) * n stays far below the bound
+    assert out["steps_within_bound"]["fp64_perturbed"] == 100
+
+
+def test_track_ends_at_a_nonfinite_step(monkeypatch):
+    monkeypatch.setattr(P, "Solver", fake_solver(lambda n: 1e-8, fail_after=35))
+    out = P.track(None, 2.5, 0.5, steps=100, every=10)
+    assert out["diverged"] == dict(solve="fp32", by_step=40)
+    assert [r["step"] for r in out["history"]] == [10, 20, 30]
