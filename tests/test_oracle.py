@@ -256,3 +256,33 @@ def test_wall_cp_of_uniform_flow_is_zero():
     cp = o.wall_cp(2, 1.4, 1.0, 2.5)
     assert cp.size == 40
     assert np.abs(cp).max() < 1e-14
+
+
+def test_frozen_limiter_steady_state_depends_on_the_state_at_the_freeze():
+    """Limiter freezing, early: a 61 x 31 wedge (M 2.8, 12 deg, Barth-Jespersen, global CFL 0.5)
+    with the limiter frozen at step 100 converges, but where it converges to depends on the
+    state the limiter values were taken from.  A relative nudge of 1e-12 to that state (far
+    below what FP32 rounding gives by then) ends more than 1e-6 away once both have converged
+    (about 4e-4 in L-inf): the amplification that leaves the FP32 and FP64 solves with early
+    freezing O(1) apart is the scheme's, not a precision's."""
+    m = H.Mesh.wedge(61, 31, theta_deg=12.0, seed=1234, numbering=H.NUMBER_RANDOM)
+    bcmap, qbc, q = H.wedge_case(2.8)
+
+    def solve(nudge):
+        o = O.Oracle(m.arrays())
+        o.gather_bcs(bcmap, qbc)
+        o.initialise(q)
+        o.set_freeze(100)
+        rng = np.random.default_rng(5)
+        res = None
+        for k in range(6000):
+            if k == 99 and nudge:
+                U = o.U()
+                o.set_U(U * (1.0 + nudge * rng.standard_normal(U.shape)))
+            _, res = o.step(O.GLOBAL_CFL, 0.5)
+        return o.U(), res
+
+    Ua, ra = solve(0.0)
+    Ub, rb = solve(1e-12)
+    assert ra < 1e-10 and rb < 1e-10                        # both converged
+    assert np.max(O.rel_linf(Ub, Ua)) > 1e-6
