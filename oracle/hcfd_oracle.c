@@ -529,6 +529,13 @@ int hcfd_oracle_set_U(hcfd_oracle* o, const double* u) {
     return 0;
 }
 
+/* Replaces the limiter values (used by the next steps only while the limiter is frozen; an
+ * unfrozen step recomputes them). */
+int hcfd_oracle_set_phi(hcfd_oracle* o, const double* phi) {
+    for (int v = 0; v < NV; v++) memcpy(o->phi[v], phi + (size_t)v*o->Nc, sizeof(double)*o->Nc);
+    return 0;
+}
+
 int hcfd_oracle_wall_cp(hcfd_oracle* o, int colour, double rho_inf, double p_inf,
                         double speed_inf, double* out) {
     if (colour < 0 || colour >= o->Ncol) return -1;

@@ -56,6 +56,8 @@ int hcfd_oracle_phase(hcfd_oracle* o, int which, double dt);
  * dt at CFL 1 for real cells, 0 for ghosts).  IV: Nc. */
 int hcfd_oracle_get(hcfd_oracle* o, int which, double* out);
 int hcfd_oracle_set_U(hcfd_oracle* o, const double* u);
+/* Replaces the limiter values, 4 x Nc variable-major (in effect while the limiter is frozen). */
+int hcfd_oracle_set_phi(hcfd_oracle* o, const double* phi);
 /* Wall pressure coefficient on the faces of one colour, in face order:
  * Cp = (p_CL - p_inf) / (0.5 rho_inf |u_inf|^2).  Returns the number of faces written. */
 int hcfd_oracle_wall_cp(hcfd_oracle* o, int colour, double rho_inf, double p_inf,

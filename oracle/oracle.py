@@ -126,6 +126,7 @@ class Oracle:
             L.hcfd_oracle_phase.argtypes = [ct.c_void_p, ct.c_int, ct.c_double]
             L.hcfd_oracle_get.argtypes = [ct.c_void_p, ct.c_int, _dp]
             L.hcfd_oracle_set_U.argtypes = [ct.c_void_p, _dp]
+            L.hcfd_oracle_set_phi.argtypes = [ct.c_void_p, _dp]
             L.hcfd_oracle_wall_cp.argtypes = [ct.c_void_p, ct.c_int, ct.c_double, ct.c_double, ct.c_double, _dp]
             L.hcfd_oracle_domain.argtypes = [ct.c_void_p] + [_dp] * 6
             L.hcfd_oracle_nreal.argtypes = [ct.c_void_p]
@@ -195,6 +196,10 @@ class Oracle:
     def set_U(self, u):
         a = np.ascontiguousarray(u, dtype=np.float64).reshape(-1)
         self.lib().hcfd_oracle_set_U(self.h, _d(a))
+
+    def set_phi(self, phi):
+        a = np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
+        self.lib().hcfd_oracle_set_phi(self.h, _d(a))
 
     def wall_cp(self, colour, rho_inf, p_inf, speed_inf):
         out = np.zeros(self.Nf)

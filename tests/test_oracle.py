@@ -286,3 +286,43 @@ def test_frozen_limiter_steady_state_depends_on_the_state_at_the_freeze():
     Ub, rb = solve(1e-12)
     assert ra < 1e-10 and rb < 1e-10                        # both converged
     assert np.max(O.rel_linf(Ub, Ua)) > 1e-6
+
+
+def test_frozen_limiter_values_rounded_to_fp32_barely_move_the_steady_state():
+    """The same wedge and freeze as above: what the converged solve is sensitive to is which
+    limiter values were frozen (a 1e-12 nudge before the freeze flips a limiter choice), not
+    their last bits nor the state after the freeze.  Rounding the frozen values and the state
+    to FP32 at the freeze step (what handing an FP64 solve over to the FP32 path does) moves
+    the converged state by less than 1e-7 (about 4e-9); a 1e-6 nudge to the state after the
+    freeze moves it by less than 1e-11."""
+    m = H.Mesh.wedge(61, 31, theta_deg=12.0, seed=1234, numbering=H.NUMBER_RANDOM)
+    bcmap, qbc, q = H.wedge_case(2.8)
+
+    def solve(at_freeze=None, after=None):
+        o = O.Oracle(m.arrays())
+        o.gather_bcs(bcmap, qbc)
+        o.initialise(q)
+        o.set_freeze(100)
+        res = None
+        for k in range(6000):
+            _, res = o.step(O.GLOBAL_CFL, 0.5)
+            if k == 99 and at_freeze:
+                at_freeze(o)
+            if k == 149 and after:
+                after(o)
+        return o.U(), res
+
+    def to_fp32(o):
+        o.set_phi(o.get(O.F_PHI).astype(np.float32).astype(np.float64))
+        o.set_U(o.U().astype(np.float32).astype(np.float64))
+
+    def nudge(o):
+        U = o.U()
+        o.set_U(U * (1.0 + 1e-6 * np.random.default_rng(5).standard_normal(U.shape)))
+
+    Ua, ra = solve()
+    Ub, rb = solve(at_freeze=to_fp32)
+    Uc, rc = solve(after=nudge)
+    assert max(ra, rb, rc) < 1e-10
+    assert np.max(O.rel_linf(Ub, Ua)) < 1e-7
+    assert np.max(O.rel_linf(Uc, Ua)) < 1e-11
