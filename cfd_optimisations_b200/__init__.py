@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import ctypes as ct
 import os
+import struct
 
 import numpy as np
 
@@ -30,7 +31,7 @@ from .native import (FIXED_DT, GLOBAL_CFL, LOCAL_CFL, FP32, FP64, KERNEL_CELL, K
 __all__ = ["Mesh", "Solver", "HcfdError", "FIXED_DT", "GLOBAL_CFL", "LOCAL_CFL", "FP32", "FP64",
            "LIMITER_BJ", "LIMITER_VENKAT", "NUMBER_NATURAL", "NUMBER_RANDOM", "NUMBER_RCM",
            "NUMBER_MORTON", "SYMMETRY", "WALL", "SUPINLET", "SUBINLET", "SUPOUTLET", "SUBOUTLET",
-           "write_hsln", "wedge_case"]
+           "write_hsln", "wedge_case", "checkpoint_info", "convert_checkpoint"]
 
 
 def _dptr(a):
@@ -261,6 +262,38 @@ def checkpoint_info(path: str) -> dict:
     _n.check(_n.lib().hcfd_checkpoint_info(os.fsencode(path), ct.byref(nc), ct.byref(prec), ct.byref(steps),
                                            ct.byref(hl)))
     return dict(Nc=nc.value, precision=prec.value, steps=steps.value, has_limiter=bool(hl.value))
+
+
+_CKPT_HEADER = struct.Struct("<8siiiiqdddii")   # magic, version, precision, Nc, has_limiter, steps, ...
+
+
+def convert_checkpoint(src: str, dst: str, precision: int) -> dict:
+    """Writes checkpoint `src` to `dst` as a checkpoint of `precision` (no GPU needed).
+    To FP32, the state and the frozen limiter values are rounded to the nearest float, as an
+    FP32 solver holds them, so the result is what that solver would have written; to FP64 the
+    values are kept (FP32 values are exact in FP64).  Restoring the result into a solver of
+    that precision, made for the same mesh with the same freezing step, hands the solve over:
+    an FP64 solve frozen at step N continues in FP32 with the FP64 solve's limiter values.
+    Returns the header of the written file (as checkpoint_info)."""
+    if precision not in (FP64, FP32):
+        raise ValueError("convert_checkpoint: precision must be FP64 or FP32")
+    info = checkpoint_info(src)
+    with open(src, "rb") as fh:
+        raw = fh.read()
+    n = 4 * info["Nc"] * (2 if info["has_limiter"] else 1)
+    if len(raw) != _CKPT_HEADER.size + 8 * n:
+        raise _n.HcfdError(_n.EIO, f"convert_checkpoint: {src} is not {n} values long")
+    head = list(_CKPT_HEADER.unpack_from(raw, 0))
+    head[2] = precision
+    vals = np.frombuffer(raw, dtype="<f8", count=n, offset=_CKPT_HEADER.size)
+    if precision == FP32:
+        vals = vals.astype(np.float32).astype("<f8")
+    tmp = dst + ".tmp"
+    with open(tmp, "wb") as fh:
+        fh.write(_CKPT_HEADER.pack(*head))
+        fh.write(np.ascontiguousarray(vals, dtype="<f8").tobytes())
+    os.replace(tmp, dst)
+    return checkpoint_info(dst)
 
 
 def plan_check(mesh: Mesh, tile: int = 0, keep_numbering: bool = False) -> dict:

@@ -16,7 +16,10 @@ the wall pressure coefficient on the lower wall, the ramp).  A third run, FP64 f
 density one rounding step larger, gives the same errors for a perturbation the size of one
 rounding: the floor that no precision can go below while the limiter keeps switching.
 With --track N the three solves instead step side by side to --max-steps, their errors
-against FP64 recorded every N steps, to show how long each stays within 1e-5.
+against FP64 recorded every N steps, to show how long each stays within 1e-5.  With
+--handoff --freeze N --track K the FP64 solve is handed over to the FP32 path at step N (its
+checkpoint converted to FP32, so the FP32 solver freezes the FP64 limiter values) and both
+that solve and an FP32 solve freezing its own values are tracked against FP64.
 """
 from __future__ import annotations
 
@@ -94,25 +97,31 @@ def _rel_l2(Ua: np.ndarray, Ub: np.ndarray) -> float:
     return float((np.sqrt(((Ua - Ub) ** 2).mean(axis=1)) / np.sqrt((Ub ** 2).mean(axis=1))).max())
 
 
-def track(mesh: Mesh, mach: float, cfl: float, steps: int, every: int, mode: int = LOCAL_CFL,
-          limiter: int = LIMITER_VENKAT, K: float = 5.0, freeze: int = 0, bound: float = 1e-5) -> dict:
-    """Steps the FP64 solve, the FP32 solve and the FP64 solve from an initial density one
-    rounding step larger side by side.  Every `every` steps it records the relative L-inf and
-    L2 errors (each the max over the conserved variables) of the last two against the first.
-    Returns the history and the last recorded step at which each L-inf error was still within
-    `bound`.  A solve that produces a NaN or Inf ends the tracking; `diverged` names it and the
-    step by which it did (the end of the interval it failed in)."""
-    bcmap, qbc, q = wedge_case(mach)
-    runs = {}
-    for name, prec, scale in (("fp64", FP64, 1.0), ("fp32", FP32, 1.0), ("fp64_perturbed", FP64, 1.0 + 2.0 ** -52)):
-        s = Solver(mesh, limiter=limiter, venkat_K=K, precision=prec, freeze_limiter_after=freeze)
-        s.gather_bcs(bcmap, qbc)
-        qi = list(q)
-        qi[0] *= scale
-        s.initialise(qi)
-        runs[name] = s
-    hist, within = [], {"fp32": 0, "fp64_perturbed": 0}
-    done, diverged = 0, None
+def _lockstep(runs: dict, others: tuple, done: int, steps: int, every: int, mode: int, cfl: float,
+              bound: float) -> dict:
+    """Steps every solve of `runs` side by side from step `done` to `steps`.  At the start and
+    every `every` steps it records the relative L-inf and L2 errors (each the max over the
+    conserved variables) of the solves named in `others` against runs["fp64"].  For each of
+    those, `steps_within_bound` is the last recorded step up to which its L-inf error stayed
+    within `bound` (None if it did not start within it).  A solve that produces a NaN or Inf
+    ends the stepping; `diverged` names it and the step by which it did (the end of the
+    interval it failed in)."""
+    hist, within, still = [], {k: None for k in others}, {k: True for k in others}
+
+    def record(step):
+        U64 = runs["fp64"].U()
+        row = dict(step=step, res_l2=runs["fp64"].stats()["res_l2"] if step else None)
+        for k in others:
+            Uk = runs[k].U()
+            row[k] = _rel_linf(Uk, U64)
+            row[k + "_l2"] = _rel_l2(Uk, U64)
+            still[k] = still[k] and row[k] <= bound
+            if still[k]:
+                within[k] = step
+        hist.append(row)
+
+    record(done)
+    diverged = None
     while done < steps:
         n = min(every, steps - done)
         for name, s in runs.items():
@@ -126,16 +135,54 @@ def track(mesh: Mesh, mach: float, cfl: float, steps: int, every: int, mode: int
         if diverged is not None:
             break
         done += n
-        U64 = runs["fp64"].U()
-        row = dict(step=done, res_l2=runs["fp64"].stats()["res_l2"])
-        for k in within:
-            Uk = runs[k].U()
-            row[k] = _rel_linf(Uk, U64)
-            row[k + "_l2"] = _rel_l2(Uk, U64)
-            if row[k] <= bound and within[k] == done - n:
-                within[k] = done
-        hist.append(row)
+        record(done)
     return dict(bound=bound, steps_within_bound=within, diverged=diverged, history=hist)
+
+
+def _solver(mesh, precision, limiter, K, freeze, mach, rho_scale=1.0):
+    bcmap, qbc, q = wedge_case(mach)
+    s = Solver(mesh, limiter=limiter, venkat_K=K, precision=precision, freeze_limiter_after=freeze)
+    s.gather_bcs(bcmap, qbc)
+    qi = list(q)
+    qi[0] *= rho_scale
+    s.initialise(qi)
+    return s
+
+
+def track(mesh: Mesh, mach: float, cfl: float, steps: int, every: int, mode: int = LOCAL_CFL,
+          limiter: int = LIMITER_VENKAT, K: float = 5.0, freeze: int = 0, bound: float = 1e-5) -> dict:
+    """Steps the FP64 solve, the FP32 solve and the FP64 solve from an initial density one
+    rounding step larger side by side from the start; the errors of the last two against the
+    first are recorded as _lockstep records them."""
+    runs = {name: _solver(mesh, prec, limiter, K, freeze, mach, scale)
+            for name, prec, scale in (("fp64", FP64, 1.0), ("fp32", FP32, 1.0),
+                                      ("fp64_perturbed", FP64, 1.0 + 2.0 ** -52))}
+    return _lockstep(runs, ("fp32", "fp64_perturbed"), 0, steps, every, mode, cfl, bound)
+
+
+def handoff(mesh: Mesh, mach: float, cfl: float, steps: int, every: int, freeze: int, mode: int = GLOBAL_CFL,
+            limiter: int = LIMITER_BJ, K: float = 5.0, bound: float = 1e-5) -> dict:
+    """An FP64 solve with the limiter frozen after step `freeze` is handed over to the FP32
+    path at that step: its checkpoint, converted to FP32 (convert_checkpoint), is restored
+    into an FP32 solver freezing after the same step, which therefore continues with the FP64
+    solve's limiter values.  Beside it an FP32 solve that ran from the start freezes its own.
+    From step `freeze` on, the three step side by side and the two FP32 solves' errors against
+    FP64 are recorded as _lockstep records them."""
+    import os
+    import tempfile
+    from . import convert_checkpoint
+    fp64 = _solver(mesh, FP64, limiter, K, freeze, mach)
+    own = _solver(mesh, FP32, limiter, K, freeze, mach)
+    fp64.step(freeze, mode, cfl)
+    own.step(freeze, mode, cfl)
+    with tempfile.TemporaryDirectory() as tmp:
+        p64, p32 = os.path.join(tmp, "fp64.ckpt"), os.path.join(tmp, "fp32.ckpt")
+        fp64.checkpoint(p64)
+        convert_checkpoint(p64, p32, FP32)
+        handed = _solver(mesh, FP32, limiter, K, freeze, mach)
+        handed.restore(p32)
+    runs = {"fp64": fp64, "fp32_handoff": handed, "fp32_own_limiter": own}
+    return _lockstep(runs, ("fp32_handoff", "fp32_own_limiter"), freeze, steps, every, mode, cfl, bound)
 
 
 def study(nx=1025, ny=513, mach=3.0, theta=20.0, cfl=0.8, orders=8.0, max_steps=50000, seed=1234,
@@ -179,9 +226,23 @@ def main():
     ap.add_argument("--track", type=int, default=0,
                     help="instead of the convergence runs: step all three solves to --max-steps and "
                          "record their errors every this many steps")
+    ap.add_argument("--handoff", action="store_true",
+                    help="with --freeze N and --track K: hand the FP64 solve over to FP32 at step N "
+                         "(FP64 limiter values) and track both FP32 solves against FP64")
     a = ap.parse_args()
     mode = GLOBAL_CFL if a.global_dt else LOCAL_CFL
     limiter = LIMITER_BJ if a.bj else LIMITER_VENKAT
+    if a.handoff:
+        if a.freeze <= 0 or a.track <= 0:
+            ap.error("--handoff needs --freeze N and --track K")
+        mesh = Mesh.wedge(a.nx, a.ny, theta_deg=a.theta, seed=1234, numbering=NUMBER_RANDOM)
+        out = handoff(mesh, a.mach, a.cfl, a.max_steps, a.track, a.freeze, mode=mode, limiter=limiter, K=a.K)
+        out["workload"] = dict(nx=a.nx, ny=a.ny, mach=a.mach, theta_deg=a.theta, cfl=a.cfl,
+                               time_mode="local" if mode == LOCAL_CFL else "global",
+                               limiter="bj" if a.bj else "venkatakrishnan", K=a.K, steps=a.max_steps,
+                               handoff_at=a.freeze)
+        print(json.dumps(out))
+        return
     if a.track:
         mesh = Mesh.wedge(a.nx, a.ny, theta_deg=a.theta, seed=1234, numbering=NUMBER_RANDOM)
         out = track(mesh, a.mach, a.cfl, a.max_steps, a.track, mode=mode, limiter=limiter, K=a.K, freeze=a.freeze)
