@@ -23,6 +23,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libhcfd_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libhcfd_ref.so")
+# where the reference sources lie when they are present (the Makefile's REF default)
+REF_DIR = os.environ.get("HCFD_REFERENCE", "/root/reference")
 
 # includes/Base/BoundaryConditions.hpp:6-13
 SYMMETRY, WALL, SUPINLET, SUBINLET, SUPOUTLET, SUBOUTLET = range(6)
@@ -45,7 +47,7 @@ def _i(a):
 
 def build(ref: bool = True) -> None:
     """Builds the oracle (and, when the reference sources exist, the reference library)."""
-    targets = ["oracle"] + (["ref"] if ref and os.path.isdir("/root/reference/src") else [])
+    targets = ["oracle"] + (["ref"] if ref and os.path.isdir(os.path.join(REF_DIR, "src")) else [])
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
