@@ -2,6 +2,7 @@
 4.1 ASCII, imported to .hmsh, loaded by the library's checked reader and stepped by the oracle;
 solutions exported to .vtu and read back."""
 import base64
+import os
 import struct
 import xml.etree.ElementTree as ET
 
@@ -13,9 +14,10 @@ from cfd_optimisations_b200 import meshio
 import oracle as O
 
 
-def write_msh(path, nx=9, ny=5, tags=(1, 2, 3, 4), untagged_curve=None):
-    """Rectangle [0,2]x[0,1]: quadrangles in the left half, triangles in the right half;
-    curves bottom, right, top, left with physical tags `tags`, the surface with tag 9."""
+def write_msh(path, nx=9, ny=5, tags=(1, 2, 3, 4), untagged_curve=None, with_quads=True):
+    """Rectangle [0,2]x[0,1]: quadrangles in the left half (none without `with_quads`), triangles in
+    the right half; curves bottom, right, top, left with physical tags `tags`, the surface with
+    tag 9."""
     xs, ys = np.linspace(0, 2, nx), np.linspace(0, 1, ny)
     nid = lambda i, j: 1 + j * nx + i
     nodes = [(nid(i, j), xs[i], ys[j]) for j in range(ny) for i in range(nx)]
@@ -23,7 +25,7 @@ def write_msh(path, nx=9, ny=5, tags=(1, 2, 3, 4), untagged_curve=None):
     for j in range(ny - 1):
         for i in range(nx - 1):
             a, b, c, d = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
-            if i < (nx - 1) // 2:
+            if with_quads and i < (nx - 1) // 2:
                 quads.append((a, b, c, d))
             else:
                 tris += [(a, b, c), (a, c, d)]
@@ -50,7 +52,7 @@ def write_msh(path, nx=9, ny=5, tags=(1, 2, 3, 4), untagged_curve=None):
     blocks, tag = [], 1
     for c in (1, 2, 3, 4):
         blocks.append((1, c, 1, sides[c]))
-    blocks += [(2, 1, 3, quads), (2, 1, 2, tris)]
+    blocks += [b for b in ((2, 1, 3, quads), (2, 1, 2, tris)) if b[3]]
     nel = sum(len(b[3]) for b in blocks)
     L += ["$Elements", f"{len(blocks)} {nel} 1 {nel}"]
     for d, e, t, els in blocks:
@@ -158,3 +160,41 @@ def test_oracle_matches_reference_on_an_imported_mixed_mesh(tmp_path):
     r.steps(50, np.array(dts))
     assert np.max(np.abs(o.U() - U0)) > 1e-2          # the walls have turned the flow
     assert np.array_equal(o.U(), r.U())
+
+
+def _canonical(m):
+    """A mesh up to its numbering: cells as (type, node coordinates); faces as (node coordinates
+    of the face, its two cells, colour name or 'interior').  A boundary face's cells are ordered
+    (interior cell, ghost); an interior face's are unordered, since which of its cells is on the
+    left follows the numbering (the lower number, in both importers)."""
+    xy = m["nodes"].reshape(-1, m["dim"])
+    node = lambda n: (float(xy[n, 0]), float(xy[n, 1]))
+    cells = [(int(m["c_ctypes"][c]), frozenset(node(n) for n in m["cn_con"][m["cn_off"][c]:m["cn_off"][c + 1]]))
+             for c in range(m["Nc"])]
+    names = ["interior"] + list(m["pnames"])
+    fn, fc, coloff = m["fn_con"].reshape(-1, 2), m["fc_con"].reshape(-1, 2), m["coloff"]
+    faces = set()
+    for col in range(m["Ncol"]):
+        for f in range(coloff[col], coloff[col + 1]):
+            pair = (cells[fc[f, 0]], cells[fc[f, 1]]) if col else frozenset((cells[fc[f, 0]], cells[fc[f, 1]]))
+            faces.add((frozenset(node(n) for n in fn[f]), pair, names[col]))
+    return sorted(cells, key=repr), faces
+
+
+def test_import_matches_the_reference_importer_up_to_numbering(tmp_path, golden):
+    """The reference's own importer (interface/Mesh.py, output committed by
+    tests/golden/make_import_golden.py) and meshio.import_msh, on the same triangle-only gmsh
+    file, give the same mesh: the same cells, the same faces with the same left/right cells
+    (the ghost on the right) and colours, the same colour names and counts.  The numbering
+    differs: the reference orders all cells, ghosts included, by one reverse Cuthill-McKee pass."""
+    write_msh(tmp_path / "t.msh", nx=9, ny=5, with_quads=False)
+    meshio.import_msh(str(tmp_path / "t.msh"), str(tmp_path / "t.hmsh"))
+    ours = O.read_hmsh(str(tmp_path / "t.hmsh"))
+    ref = O.read_hmsh(os.path.join(golden, "ref_import_tri.hmsh"))
+    for k in ("dim", "Nn", "Nc", "Nf", "Ncol", "NBCcol", "pnames"):
+        assert ours[k] == ref[k], k
+    assert np.array_equal(np.diff(ours["coloff"]), np.diff(ref["coloff"]))
+    cells_a, faces_a = _canonical(ours)
+    cells_b, faces_b = _canonical(ref)
+    assert cells_a == cells_b
+    assert faces_a == faces_b and len(faces_a) == ours["Nf"]
