@@ -1,8 +1,12 @@
-"""Regenerates ref_import_tri.hmsh: the reference's own gmsh importer (interface/Mesh.py,
-Mesh.generate_from_msh + write_hmsh, imported from the reference sources unchanged) run on
-the triangle-only rectangle that tests/test_meshio.py writes (write_msh(nx=9, ny=5,
-with_quads=False): 64 triangles, curves tagged 1..4).  Run in a container that has the reference
-sources:
+"""Regenerates the reference's own gmsh importer's outputs (interface/Mesh.py,
+Mesh.generate_from_msh + write_hmsh, imported from the reference sources unchanged):
+
+* ref_import_tri.hmsh — on the triangle-only rectangle that tests/test_meshio.py writes
+  (write_msh(nx=9, ny=5, with_quads=False): 64 triangles, curves tagged 1..4);
+* ref_import_wedge.hmsh — on the library's generated wedge (13 x 7 nodes, seed 3, random
+  numbering) written as gmsh by write_msh_of_mesh (boundary colour k as curve tag k).
+
+Run in a container that has the reference sources:
 
     python tests/golden/make_import_golden.py
 
@@ -38,7 +42,8 @@ def reference_mesh_module():
 
 
 def main():
-    from test_meshio import write_msh
+    import cfd_optimisations_b200 as H
+    from test_meshio import write_msh, write_msh_of_mesh
     R = reference_mesh_module()
     with tempfile.TemporaryDirectory() as tmp:
         src = os.path.join(tmp, "tri.msh")
@@ -46,6 +51,11 @@ def main():
         m = R.Mesh()
         m.generate_from_msh(src)
         m.write_hmsh(os.path.join(HERE, "ref_import_tri.hmsh"))
+        src = os.path.join(tmp, "wedge.msh")
+        write_msh_of_mesh(src, H.Mesh.wedge(13, 7, seed=3, numbering=H.NUMBER_RANDOM).arrays())
+        m = R.Mesh()
+        m.generate_from_msh(src)
+        m.write_hmsh(os.path.join(HERE, "ref_import_wedge.hmsh"))
 
 
 if __name__ == "__main__":

@@ -14,13 +14,48 @@ from cfd_optimisations_b200 import meshio
 import oracle as O
 
 
+def _msh_text(xy, curves, quads, tris, untagged_curve=None):
+    """gmsh 4.1 ASCII text: nodes 1..len(xy); curve c (1-based) of `curves` = (physical tag,
+    name, line elements) as an entity with that tag (none for `untagged_curve`); quadrangles
+    and triangles (node tags) in one surface with physical tag 9 "domain", named last."""
+    n = len(curves)
+    L = ["$MeshFormat", "4.1 0 8", "$EndMeshFormat", "$PhysicalNames", str(n + 1)]
+    for tag, name, _ in curves:
+        L.append(f'1 {tag} "{name}"')
+    L.append('2 9 "domain"')
+    L += ["$EndPhysicalNames", "$Entities", f"4 {n} 1 0"]
+    for p in range(1, 5):
+        L.append(f"{p} 0 0 0 0")
+    for c, (tag, _, _) in enumerate(curves, 1):
+        ph = "0" if c == untagged_curve else f"1 {tag}"
+        L.append(f"{c} 0 0 0 2 1 0 {ph} 2 {c} {-(c % 4 + 1)}")
+    L.append(f"1 0 0 0 2 1 0 1 9 {n} " + " ".join(str(c) for c in range(1, n + 1)))
+    L += ["$EndEntities", "$Nodes", f"1 {len(xy)} 1 {len(xy)}", f"2 1 0 {len(xy)}"]
+    L += [str(t) for t in range(1, len(xy) + 1)]
+    L += [f"{float(x)!r} {float(y)!r} 0" for x, y in xy]
+    L.append("$EndNodes")
+    blocks, tag = [], 1
+    for c, (_, _, lines) in enumerate(curves, 1):
+        blocks.append((1, c, 1, lines))
+    blocks += [b for b in ((2, 1, 3, quads), (2, 1, 2, tris)) if len(b[3])]
+    nel = sum(len(b[3]) for b in blocks)
+    L += ["$Elements", f"{len(blocks)} {nel} 1 {nel}"]
+    for d, e, t, els in blocks:
+        L.append(f"{d} {e} {t} {len(els)}")
+        for el in els:
+            L.append(" ".join(str(x) for x in (tag,) + tuple(el)))
+            tag += 1
+    L.append("$EndElements")
+    return "\n".join(L) + "\n"
+
+
 def write_msh(path, nx=9, ny=5, tags=(1, 2, 3, 4), untagged_curve=None, with_quads=True):
     """Rectangle [0,2]x[0,1]: quadrangles in the left half (none without `with_quads`), triangles in
     the right half; curves bottom, right, top, left with physical tags `tags`, the surface with
     tag 9."""
     xs, ys = np.linspace(0, 2, nx), np.linspace(0, 1, ny)
     nid = lambda i, j: 1 + j * nx + i
-    nodes = [(nid(i, j), xs[i], ys[j]) for j in range(ny) for i in range(nx)]
+    xy = [(xs[i], ys[j]) for j in range(ny) for i in range(nx)]
     quads, tris = [], []
     for j in range(ny - 1):
         for i in range(nx - 1):
@@ -34,36 +69,28 @@ def write_msh(path, nx=9, ny=5, tags=(1, 2, 3, 4), untagged_curve=None, with_qua
              3: [(nid(i + 1, ny - 1), nid(i, ny - 1)) for i in range(nx - 1)],
              4: [(nid(0, j + 1), nid(0, j)) for j in range(ny - 1)]}
     names = {1: "lower", 2: "outlet", 3: "upper", 4: "inlet"}
-    L = ["$MeshFormat", "4.1 0 8", "$EndMeshFormat", "$PhysicalNames", "5"]
-    for c in (1, 2, 3, 4):
-        L.append(f'1 {tags[c - 1]} "{names[c]}"')
-    L.append('2 9 "domain"')
-    L += ["$EndPhysicalNames", "$Entities", "4 4 1 0"]
-    for p in range(1, 5):
-        L.append(f"{p} 0 0 0 0")
-    for c in (1, 2, 3, 4):
-        ph = "0" if c == untagged_curve else f"1 {tags[c - 1]}"
-        L.append(f"{c} 0 0 0 2 1 0 {ph} 2 {c} {-(c % 4 + 1)}")
-    L.append("1 0 0 0 2 1 0 1 9 4 1 2 3 4")
-    L += ["$EndEntities", "$Nodes", f"1 {len(nodes)} 1 {len(nodes)}", f"2 1 0 {len(nodes)}"]
-    L += [str(t) for t, _, _ in nodes]
-    L += [f"{float(x)!r} {float(y)!r} 0" for _, x, y in nodes]
-    L.append("$EndNodes")
-    blocks, tag = [], 1
-    for c in (1, 2, 3, 4):
-        blocks.append((1, c, 1, sides[c]))
-    blocks += [b for b in ((2, 1, 3, quads), (2, 1, 2, tris)) if b[3]]
-    nel = sum(len(b[3]) for b in blocks)
-    L += ["$Elements", f"{len(blocks)} {nel} 1 {nel}"]
-    for d, e, t, els in blocks:
-        L.append(f"{d} {e} {t} {len(els)}")
-        for el in els:
-            L.append(" ".join(str(x) for x in (tag,) + tuple(el)))
-            tag += 1
-    L.append("$EndElements")
+    curves = [(tags[c - 1], names[c], sides[c]) for c in (1, 2, 3, 4)]
     with open(path, "w") as fh:
-        fh.write("\n".join(L) + "\n")
+        fh.write(_msh_text(xy, curves, quads, tris, untagged_curve))
     return dict(nquads=len(quads), ntris=len(tris), nlines=sum(len(v) for v in sides.values()))
+
+
+def write_msh_of_mesh(path, m):
+    """A library mesh (Mesh.arrays()) as gmsh: its real cells as surface elements, each
+    boundary colour k (1-based) as a curve with physical tag k and the colour's name whose line
+    elements are that colour's ghost cells (two nodes each)."""
+    xy = m["nodes"].reshape(-1, 2)
+    cn_off, cn_con = m["cn_off"], m["cn_con"]
+    fc, coloff = m["fc_con"].reshape(-1, 2), m["coloff"]
+    cell = lambda c: tuple(int(n) + 1 for n in cn_con[cn_off[c]:cn_off[c + 1]])
+    ghosts = set(int(g) for g in fc[coloff[1]:, 1])
+    real = [c for c in range(m["Nc"]) if c not in ghosts]
+    curves = [(k, m["pnames"][k - 1], [cell(fc[f, 1]) for f in range(coloff[k], coloff[k + 1])])
+              for k in range(1, m["Ncol"])]
+    quads = [cell(c) for c in real if cn_off[c + 1] - cn_off[c] == 4]
+    tris = [cell(c) for c in real if cn_off[c + 1] - cn_off[c] == 3]
+    with open(path, "w") as fh:
+        fh.write(_msh_text([tuple(p) for p in xy], curves, quads, tris))
 
 
 def test_import_builds_a_valid_mesh(tmp_path):
@@ -163,13 +190,13 @@ def test_oracle_matches_reference_on_an_imported_mixed_mesh(tmp_path):
 
 
 def _canonical(m):
-    """A mesh up to its numbering: cells as (type, node coordinates); faces as (node coordinates
+    """A mesh up to its numbering: cells as (node count, node coordinates); faces as (node coordinates
     of the face, its two cells, colour name or 'interior').  A boundary face's cells are ordered
     (interior cell, ghost); an interior face's are unordered, since which of its cells is on the
     left follows the numbering (the lower number, in both importers)."""
     xy = m["nodes"].reshape(-1, m["dim"])
     node = lambda n: (float(xy[n, 0]), float(xy[n, 1]))
-    cells = [(int(m["c_ctypes"][c]), frozenset(node(n) for n in m["cn_con"][m["cn_off"][c]:m["cn_off"][c + 1]]))
+    cells = [(int(m["cn_off"][c + 1] - m["cn_off"][c]), frozenset(node(n) for n in m["cn_con"][m["cn_off"][c]:m["cn_off"][c + 1]]))
              for c in range(m["Nc"])]
     names = ["interior"] + list(m["pnames"])
     fn, fc, coloff = m["fn_con"].reshape(-1, 2), m["fc_con"].reshape(-1, 2), m["coloff"]
@@ -198,3 +225,19 @@ def test_import_matches_the_reference_importer_up_to_numbering(tmp_path, golden)
     cells_b, faces_b = _canonical(ref)
     assert cells_a == cells_b
     assert faces_a == faces_b and len(faces_a) == ours["Nf"]
+
+
+def test_generated_wedge_matches_the_reference_importer_up_to_numbering(golden):
+    """The wedge generator's mesh (13 x 7 nodes, seed 3, random numbering), written as gmsh and
+    imported by the reference's own importer (output committed by
+    tests/golden/make_import_golden.py), is the same mesh: the generator builds its cells, faces,
+    boundary orientation and colours as the reference's mesh pipeline does."""
+    m = H.Mesh.wedge(13, 7, seed=3, numbering=H.NUMBER_RANDOM).arrays()
+    ref = O.read_hmsh(os.path.join(golden, "ref_import_wedge.hmsh"))
+    for k in ("dim", "Nn", "Nc", "Nf", "Ncol", "NBCcol", "pnames"):
+        assert m[k] == ref[k], k
+    assert np.array_equal(np.diff(m["coloff"]), np.diff(ref["coloff"]))
+    cells_a, faces_a = _canonical(m)
+    cells_b, faces_b = _canonical(ref)
+    assert cells_a == cells_b
+    assert faces_a == faces_b and len(faces_a) == m["Nf"]
