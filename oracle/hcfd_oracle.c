@@ -15,6 +15,22 @@
 #define NV 4
 #define ND 2
 
+/* The arithmetic of the step (state, gradients, limiter values, fluxes, residuals).  The
+ * default build is double and restates the reference.  The HCFD_ORACLE_FP32 build is the CPU
+ * counterpart of the library's FP32 path: geometry computed in double and rounded once,
+ * state and step arithmetic in IEEE float, each cell's residual summed with a compensated
+ * two-sum in the reference's face order, dt minima and the residual norm in double.  (The
+ * library's FP32 kernels use the hardware's approximate division and square root, so the two
+ * agree to a few units in the last place per operation, not bit for bit.) */
+#ifdef HCFD_ORACLE_FP32
+typedef float real;
+#define RSQRT sqrtf
+#else
+typedef double real;
+#define RSQRT sqrt
+#endif
+#define RL(x) ((real) (x))
+
 struct hcfd_oracle {
     int Nn, Nc, Nf, Ncol, NBC, F_BC, nreal;
     double gma;
@@ -28,10 +44,13 @@ struct hcfd_oracle {
     double* Af; double* If;
     double* xc;   /* [Nc][2]    */
     double* iv;
+    /* the geometry in the step's arithmetic (the arrays above in the double build) */
+    real* rfR; real* nfR; real* AfR; real* IfR; real* ivR;
     /* Euler state (src/Base/Euler.cpp:9-15) */
-    double* U[NV]; double* Q[NV]; double* R[NV]; double* phi[NV]; double* G[NV];
-    double* Umin; double* Umax; double* dL; double* dR;
-    double* dtloc;
+    real* U[NV]; real* Q[NV]; real* R[NV]; real* phi[NV]; real* G[NV];
+    real* Rc[NV];  /* compensation terms of the two-sums (float build) */
+    real* Umin; real* Umax; real* dL; real* dR;
+    real* dtloc;
     /* BCs */
     int* bc_type; int* bc_F1; int* bc_F2;
     double (*QBC)[NV]; double (*UBC)[NV];
@@ -40,6 +59,18 @@ struct hcfd_oracle {
 };
 
 static inline double dot2(const double* a, const double* b) { return a[0]*b[0] + a[1]*b[1]; }
+static inline real dot2r(const real* a, const real* b) { return a[0]*b[0] + a[1]*b[1]; }
+
+#ifdef HCFD_ORACLE_FP32
+/* s + c += x (Knuth's two-sum); the library's FP32 path accumulates each cell's residual so. */
+static inline void two_sum(real* s, real* c, real x) {
+    real t = *s + x;
+    real bp = t - *s;
+    real e = (*s - (t - bp)) + (x - bp);
+    *s = t;
+    *c += e;
+}
+#endif
 
 /* Domain::compute_xf / compute_xc / compute_rf / compute_nf / compute_If / compute_iv
  * (src/Base/Domain.cpp:44-146) and zero_bc_iv (:148-154, called by the Euler constructor,
@@ -124,23 +155,37 @@ hcfd_oracle* hcfd_oracle_create(int Nn, int Nc, int Nf, int Ncol, int NBCcol,
     o->xc = (double*) xcalloc((size_t)2*Nc, sizeof(double));
     o->iv = (double*) xcalloc(Nc, sizeof(double));
     for (int v = 0; v < NV; v++) {
-        o->U[v] = (double*) xcalloc(Nc, sizeof(double));
-        o->Q[v] = (double*) xcalloc(Nc, sizeof(double));
-        o->R[v] = (double*) xcalloc(Nc, sizeof(double));
-        o->phi[v] = (double*) xcalloc(Nc, sizeof(double));
-        o->G[v] = (double*) xcalloc((size_t)2*Nc, sizeof(double));
+        o->U[v] = (real*) xcalloc(Nc, sizeof(real));
+        o->Q[v] = (real*) xcalloc(Nc, sizeof(real));
+        o->R[v] = (real*) xcalloc(Nc, sizeof(real));
+        o->Rc[v] = (real*) xcalloc(Nc, sizeof(real));
+        o->phi[v] = (real*) xcalloc(Nc, sizeof(real));
+        o->G[v] = (real*) xcalloc((size_t)2*Nc, sizeof(real));
     }
-    o->Umin = (double*) xcalloc(Nc, sizeof(double));
-    o->Umax = (double*) xcalloc(Nc, sizeof(double));
-    o->dL = (double*) xcalloc(Nf, sizeof(double));
-    o->dR = (double*) xcalloc(Nf, sizeof(double));
-    o->dtloc = (double*) xcalloc(Nc, sizeof(double));
+    o->Umin = (real*) xcalloc(Nc, sizeof(real));
+    o->Umax = (real*) xcalloc(Nc, sizeof(real));
+    o->dL = (real*) xcalloc(Nf, sizeof(real));
+    o->dR = (real*) xcalloc(Nf, sizeof(real));
+    o->dtloc = (real*) xcalloc(Nc, sizeof(real));
     o->bc_type = (int*) xcalloc(NBCcol, sizeof(int));
     o->bc_F1 = (int*) xcalloc(NBCcol, sizeof(int));
     o->bc_F2 = (int*) xcalloc(NBCcol, sizeof(int));
     o->QBC = (double (*)[NV]) xcalloc(NBCcol, sizeof(double[NV]));
     o->UBC = (double (*)[NV]) xcalloc(NBCcol, sizeof(double[NV]));
     build_domain(o);
+#ifdef HCFD_ORACLE_FP32
+    o->rfR = (real*) xcalloc((size_t)4*Nf, sizeof(real));
+    o->nfR = (real*) xcalloc((size_t)2*Nf, sizeof(real));
+    o->AfR = (real*) xcalloc(Nf, sizeof(real));
+    o->IfR = (real*) xcalloc(Nf, sizeof(real));
+    o->ivR = (real*) xcalloc(Nc, sizeof(real));
+    for (size_t k = 0; k < (size_t)4*Nf; k++) o->rfR[k] = RL(o->rf[k]);
+    for (size_t k = 0; k < (size_t)2*Nf; k++) o->nfR[k] = RL(o->nf[k]);
+    for (int f = 0; f < Nf; f++) { o->AfR[f] = RL(o->Af[f]); o->IfR[f] = RL(o->If[f]); }
+    for (int i = 0; i < Nc; i++) o->ivR[i] = RL(o->iv[i]);
+#else
+    o->rfR = o->rf; o->nfR = o->nf; o->AfR = o->Af; o->IfR = o->If; o->ivR = o->iv;
+#endif
     o->nreal = 0;
     for (int i = 0; i < Nc; i++) o->nreal += (o->iv[i] != 0.0);
     return o;
@@ -151,7 +196,12 @@ void hcfd_oracle_free(hcfd_oracle* o) {
     free(o->coltag); free(o->coloff); free(o->nodes); free(o->fn_con); free(o->fc_con);
     free(o->cn_off); free(o->cn_con); free(o->rf); free(o->xf); free(o->nf); free(o->Af);
     free(o->If); free(o->xc); free(o->iv);
-    for (int v = 0; v < NV; v++) { free(o->U[v]); free(o->Q[v]); free(o->R[v]); free(o->phi[v]); free(o->G[v]); }
+    for (int v = 0; v < NV; v++) {
+        free(o->U[v]); free(o->Q[v]); free(o->R[v]); free(o->Rc[v]); free(o->phi[v]); free(o->G[v]);
+    }
+#ifdef HCFD_ORACLE_FP32
+    free(o->rfR); free(o->nfR); free(o->AfR); free(o->IfR); free(o->ivR);
+#endif
     free(o->Umin); free(o->Umax); free(o->dL); free(o->dR); free(o->dtloc);
     free(o->bc_type); free(o->bc_F1); free(o->bc_F2); free(o->QBC); free(o->UBC);
     free(o);
@@ -186,17 +236,17 @@ int hcfd_oracle_gather_bcs(hcfd_oracle* o, const int* bcmap, int nbcmap, const d
 
 /* update_cells of each BC type, in BC order (src/Base/Euler.cpp:138-142). */
 static void update_bc_cells(hcfd_oracle* o) {
-    double** U = o->U;
+    real** U = o->U;
     const double gma = o->gma;
     for (int bc = 0; bc < o->NBC; bc++) {
         for (int f = o->bc_F1[bc]; f < o->bc_F2[bc]; f++) {
             int CL = o->fc_con[2*f], CR = o->fc_con[2*f+1];
             switch (o->bc_type[bc]) {
             case 0: {                                   /* Symmetry.cpp:5-24 */
-                const double* n = &o->nf[2*f];
-                double ul[ND];
+                const real* n = &o->nfR[2*f];
+                real ul[ND];
                 for (int d = 0; d < ND; d++) ul[d] = U[d+1][CL];
-                double nor = dot2(ul, n);
+                real nor = dot2r(ul, n);
                 U[0][CR] = U[0][CL];
                 for (int d = 0; d < ND; d++) U[d+1][CR] = ul[d] - 2*nor*n[d];
                 U[ND+1][CR] = U[ND+1][CL];
@@ -207,14 +257,14 @@ static void update_bc_cells(hcfd_oracle* o) {
                 U[ND+1][CR] = U[ND+1][CL];
                 break;
             case 2:                                     /* Inlet.cpp:4-13 */
-                for (int v = 0; v < NV; v++) U[v][CR] = o->UBC[bc][v];
+                for (int v = 0; v < NV; v++) U[v][CR] = RL(o->UBC[bc][v]);
                 break;
             case 3: {                                   /* Inlet.cpp:15-31 */
-                double UL[NV];
+                real UL[NV];
                 for (int v = 0; v < NV; v++) UL[v] = U[v][CL];
-                double PL = (gma-1)*(UL[ND+1] - 0.5*dot2(&UL[1], &UL[1])/UL[0]);
-                for (int v = 0; v < NV; v++) U[v][CR] = o->UBC[bc][v];
-                U[ND+1][CR] = PL/(gma-1) + 0.5*o->QBC[bc][0]*dot2(&o->QBC[bc][1], &o->QBC[bc][1]);
+                real PL = RL(gma-1)*(UL[ND+1] - RL(0.5)*dot2r(&UL[1], &UL[1])/UL[0]);
+                for (int v = 0; v < NV; v++) U[v][CR] = RL(o->UBC[bc][v]);
+                U[ND+1][CR] = PL/RL(gma-1) + RL(0.5*o->QBC[bc][0]*dot2(&o->QBC[bc][1], &o->QBC[bc][1]));
             } break;
             case 4:                                     /* Outlet.cpp:4-13 */
                 for (int v = 0; v < NV; v++) U[v][CR] = U[v][CL];
@@ -223,12 +273,12 @@ static void update_bc_cells(hcfd_oracle* o) {
                 /* The reference's loop (Outlet.cpp:26-28) reads rul[-1] (undefined) and
                  * stops one momentum component short.  Restated as a subsonic outlet that
                  * takes rho and rho*u from the interior and p from the BC state. */
-                double rl = U[0][CL];
-                double rul[ND];
+                real rl = U[0][CL];
+                real rul[ND];
                 for (int d = 0; d < ND; d++) rul[d] = U[d+1][CL];
                 U[0][CR] = rl;
                 for (int d = 0; d < ND; d++) U[d+1][CR] = rul[d];
-                U[ND+1][CR] = o->QBC[bc][ND+1]/(gma-1) + 0.5*dot2(rul, rul)/rl;
+                U[ND+1][CR] = RL(o->QBC[bc][ND+1]/(gma-1)) + RL(0.5)*dot2r(rul, rul)/rl;
             } break;
             }
         }
@@ -239,7 +289,7 @@ int hcfd_oracle_initialise(hcfd_oracle* o, const double* qic) {
     double UIC[NV];
     prim_to_cons(qic, o->gma, UIC);
     for (int v = 0; v < NV; v++)
-        for (int i = 0; i < o->Nc; i++) o->U[v][i] = UIC[v];
+        for (int i = 0; i < o->Nc; i++) o->U[v][i] = RL(UIC[v]);
     update_bc_cells(o);
     o->nsteps = 0;
     return 0;
@@ -262,40 +312,40 @@ int hcfd_oracle_set_limiter(hcfd_oracle* o, int kind, double K) {
 /* GaussGreen::compute_gradient (src/Base/GaussGreen.cpp:14-40). */
 static void gradient(hcfd_oracle* o) {
     const int Nc = o->Nc, Nf = o->Nf;
-    for (int v = 0; v < NV; v++) memset(o->G[v], 0, sizeof(double)*2*Nc);
+    for (int v = 0; v < NV; v++) memset(o->G[v], 0, sizeof(real)*2*Nc);
     for (int f = 0; f < Nf; f++) {
         int CL = o->fc_con[2*f], CR = o->fc_con[2*f+1];
         for (int v = 0; v < NV; v++) {
             for (int d = 0; d < ND; d++) {
-                double uf = o->U[v][CL]*o->If[f] + o->U[v][CR]*(1-o->If[f]);
-                o->G[v][d*Nc+CL] += uf*o->Af[f]*o->nf[2*f+d];
-                o->G[v][d*Nc+CR] -= uf*o->Af[f]*o->nf[2*f+d];
+                real uf = o->U[v][CL]*o->IfR[f] + o->U[v][CR]*(1-o->IfR[f]);
+                o->G[v][d*Nc+CL] += uf*o->AfR[f]*o->nfR[2*f+d];
+                o->G[v][d*Nc+CR] -= uf*o->AfR[f]*o->nfR[2*f+d];
             }
         }
     }
     for (int v = 0; v < NV; v++)
         for (int d = 0; d < ND; d++)
-            for (int i = 0; i < Nc; i++) o->G[v][d*Nc+i] *= o->iv[i];
+            for (int i = 0; i < Nc; i++) o->G[v][d*Nc+i] *= o->ivR[i];
 }
 
 /* One side of a face for the Venkatakrishnan limiter: d = grad.r, D1 = Umax-U or Umin-U,
  * eps2 = (K h)^3 with h = sqrt(cell area).
  *   phi = min(1, (D1^2 + eps2 + 2 D1 d) / (D1^2 + 2 d^2 + D1 d + eps2)). */
-static inline double venkat(double D1, double d, double eps2) {
-    double num = D1*D1 + eps2 + 2.0*D1*d;
-    double den = D1*D1 + 2.0*d*d + D1*d + eps2;
+static inline real venkat(real D1, real d, real eps2) {
+    real num = D1*D1 + eps2 + RL(2)*D1*d;
+    real den = D1*D1 + RL(2)*d*d + D1*d + eps2;
     return fmin(1, num/den);
 }
 
 /* Limiter::limit_gradient (src/Base/Limiter.cpp:19-77); the Venkatakrishnan branch replaces
  * the Barth-Jespersen ratio with venkat() and keeps everything else. */
 static void limiter(hcfd_oracle* o) {
-    const double eps = 1e-9;
+    const real eps = RL(1e-9);
     const int Nf = o->Nf, Nc = o->Nc;
-    double GL[ND], GR[ND];
+    real GL[ND], GR[ND];
     for (int v = 0; v < NV; v++) {
-        memcpy(o->Umin, o->U[v], Nc*sizeof(double));
-        memcpy(o->Umax, o->U[v], Nc*sizeof(double));
+        memcpy(o->Umin, o->U[v], Nc*sizeof(real));
+        memcpy(o->Umax, o->U[v], Nc*sizeof(real));
         for (int i = 0; i < Nc; i++) o->phi[v][i] = 1.0;
         for (int f = 0; f < Nf; f++) {
             int CL = o->fc_con[2*f], CR = o->fc_con[2*f+1];
@@ -307,23 +357,23 @@ static void limiter(hcfd_oracle* o) {
         for (int f = 0; f < Nf; f++) {
             int CL = o->fc_con[2*f], CR = o->fc_con[2*f+1];
             for (int d = 0; d < ND; d++) { GL[d] = o->G[v][d*Nc+CL]; GR[d] = o->G[v][d*Nc+CR]; }
-            o->dL[f] = dot2(GL, &o->rf[4*f]);
-            o->dR[f] = dot2(GR, &o->rf[4*f+2]);
+            o->dL[f] = dot2r(GL, &o->rfR[4*f]);
+            o->dR[f] = dot2r(GR, &o->rfR[4*f+2]);
         }
         for (int f = 0; f < Nf; f++) {
             int CL = o->fc_con[2*f], CR = o->fc_con[2*f+1];
-            double UL = o->U[v][CL], UR = o->U[v][CR];
-            double phi_fl = 1.0, phi_fr = 1.0;
-            double dLf = o->dL[f], dRf = o->dR[f];
+            real UL = o->U[v][CL], UR = o->U[v][CR];
+            real phi_fl = 1.0, phi_fr = 1.0;
+            real dLf = o->dL[f], dRf = o->dR[f];
             if (o->limiter == HCFD_OR_BJ) {
                 phi_fl = (dLf >  eps) ? fmin(1, (o->Umax[CL]-UL)/dLf) : phi_fl;
                 phi_fl = (dLf < -eps) ? fmin(1, (o->Umin[CL]-UL)/dLf) : phi_fl;
                 phi_fr = (dRf >  eps) ? fmin(1, (o->Umax[CR]-UR)/dRf) : phi_fr;
                 phi_fr = (dRf < -eps) ? fmin(1, (o->Umin[CR]-UR)/dRf) : phi_fr;
             } else {
-                double kL = o->iv[CL] != 0.0 ? o->K*sqrt(1.0/o->iv[CL]) : 0.0;
-                double kR = o->iv[CR] != 0.0 ? o->K*sqrt(1.0/o->iv[CR]) : 0.0;
-                double eL = kL*kL*kL, eR = kR*kR*kR;
+                real kL = o->ivR[CL] != 0 ? RL(o->K)*RSQRT(RL(1.0)/o->ivR[CL]) : RL(0.0);
+                real kR = o->ivR[CR] != 0 ? RL(o->K)*RSQRT(RL(1.0)/o->ivR[CR]) : RL(0.0);
+                real eL = kL*kL*kL, eR = kR*kR*kR;
                 phi_fl = (dLf >  eps) ? venkat(o->Umax[CL]-UL, dLf, eL) : phi_fl;
                 phi_fl = (dLf < -eps) ? venkat(o->Umin[CL]-UL, dLf, eL) : phi_fl;
                 phi_fr = (dRf >  eps) ? venkat(o->Umax[CR]-UR, dRf, eR) : phi_fr;
@@ -354,10 +404,10 @@ static void bc_grads_limiter(hcfd_oracle* o) {
 }
 
 /* Flux::EulerFlux (src/Base/Flux.cpp:89-97). */
-static inline void euler_flux(const double U[NV], const double n[ND], double gma, double F[NV]) {
-    double gmo = gma-1;
-    double ir = 1.0/U[0];
-    double P = gmo* (U[ND+1] - 0.5*ir*dot2(&U[1],&U[1]));
+static inline void euler_flux(const real U[NV], const real n[ND], real gma, real F[NV]) {
+    real gmo = gma-1;
+    real ir = RL(1.0)/U[0];
+    real P = gmo* (U[ND+1] - RL(0.5)*ir*dot2r(&U[1],&U[1]));
     F[0] = n[0]* U[1]              + n[1]* U[2]             ;
     F[1] = n[0]*(U[1]*U[1]*ir + P) + n[1]* U[2]*U[1]*ir     ;
     F[2] = n[0]* U[1]*U[2]*ir      + n[1]*(U[2]*U[2]*ir + P);
@@ -365,53 +415,63 @@ static inline void euler_flux(const double U[NV], const double n[ND], double gma
 }
 
 /* Flux::Rusanov (src/Base/Flux.cpp:52-81). */
-static inline void rusanov(const double UL[NV], const double UR[NV], const double n[ND],
-                           double gma, double F[NV]) {
-    double gmo = gma-1;
-    double irl = 1.0/UL[0];
-    double irr = 1.0/UR[0];
-    double nvl = dot2(n, &UL[1])*irl;
-    double nvr = dot2(n, &UR[1])*irr;
-    double qql = 0.5*dot2(&UL[1], &UL[1])*irl;
-    double qqr = 0.5*dot2(&UR[1], &UR[1])*irr;
-    double pl  = gmo*(UL[ND+1] - qql);
-    double pr  = gmo*(UR[ND+1] - qqr);
-    double al  = sqrt(gma*pl*irl);
-    double ar  = sqrt(gma*pr*irr);
-    double S1  = fmax(fabs(nvl-al), fabs(nvr-ar));
-    double S2  = fmax(fabs(nvl+al), fabs(nvr+ar));
-    double S   = fmax(S1, S2);
-    double FL[NV], FR[NV];
+static inline void rusanov(const real UL[NV], const real UR[NV], const real n[ND],
+                           real gma, real F[NV]) {
+    real gmo = gma-1;
+    real irl = RL(1.0)/UL[0];
+    real irr = RL(1.0)/UR[0];
+    real nvl = dot2r(n, &UL[1])*irl;
+    real nvr = dot2r(n, &UR[1])*irr;
+    real qql = RL(0.5)*dot2r(&UL[1], &UL[1])*irl;
+    real qqr = RL(0.5)*dot2r(&UR[1], &UR[1])*irr;
+    real pl  = gmo*(UL[ND+1] - qql);
+    real pr  = gmo*(UR[ND+1] - qqr);
+    real al  = RSQRT(gma*pl*irl);
+    real ar  = RSQRT(gma*pr*irr);
+    real S1  = fmax(fabs(nvl-al), fabs(nvr-ar));
+    real S2  = fmax(fabs(nvl+al), fabs(nvr+ar));
+    real S   = fmax(S1, S2);
+    real FL[NV], FR[NV];
     euler_flux(UL, n, gma, FL);
     euler_flux(UR, n, gma, FR);
-    for (int v = 0; v < NV; v++) F[v] = 0.5 * ( (FL[v] + FR[v]) - S*(UR[v] - UL[v]) );
+    for (int v = 0; v < NV; v++) F[v] = RL(0.5) * ( (FL[v] + FR[v]) - S*(UR[v] - UL[v]) );
 }
 
 /* Flux::ComputeFlux with Flux::MUSCL (src/Base/Flux.cpp:9-50, 83-87). */
 static void flux(hcfd_oracle* o) {
     const int Nc = o->Nc, Nf = o->Nf;
-    double UL[NV], UR[NV], phiL[NV], phiR[NV], GL[NV][ND], GR[NV][ND];
-    double UfL[NV], UfR[NV], Ff[NV];
+    real UL[NV], UR[NV], phiL[NV], phiR[NV], GL[NV][ND], GR[NV][ND];
+    real UfL[NV], UfR[NV], Ff[NV];
     for (int f = 0; f < Nf; f++) {
         int CL = o->fc_con[2*f], CR = o->fc_con[2*f+1];
-        double Af = o->Af[f];
+        real Af = o->AfR[f];
         for (int v = 0; v < NV; v++) {
             UL[v] = o->U[v][CL]; UR[v] = o->U[v][CR];
             phiL[v] = o->phi[v][CL]; phiR[v] = o->phi[v][CR];
             for (int d = 0; d < ND; d++) { GL[v][d] = o->G[v][d*Nc+CL]; GR[v][d] = o->G[v][d*Nc+CR]; }
         }
-        const double* rL = &o->rf[4*f];
-        const double* rR = &o->rf[4*f+2];
-        for (int v = 0; v < NV; v++) UfL[v] = UL[v] + phiL[v]*dot2(GL[v], rL);
-        for (int v = 0; v < NV; v++) UfR[v] = UR[v] + phiR[v]*dot2(GR[v], rR);
-        rusanov(UfL, UfR, &o->nf[2*f], o->gma, Ff);
+        const real* rL = &o->rfR[4*f];
+        const real* rR = &o->rfR[4*f+2];
+        for (int v = 0; v < NV; v++) UfL[v] = UL[v] + phiL[v]*dot2r(GL[v], rL);
+        for (int v = 0; v < NV; v++) UfR[v] = UR[v] + phiR[v]*dot2r(GR[v], rR);
+        rusanov(UfL, UfR, &o->nfR[2*f], RL(o->gma), Ff);
         for (int v = 0; v < NV; v++) {
+#ifdef HCFD_ORACLE_FP32
+            two_sum(&o->R[v][CL], &o->Rc[v][CL], -(Af*Ff[v]));
+            two_sum(&o->R[v][CR], &o->Rc[v][CR], Af*Ff[v]);
+#else
             o->R[v][CL] -= Af*Ff[v];
             o->R[v][CR] += Af*Ff[v];
+#endif
         }
     }
+#ifdef HCFD_ORACLE_FP32
+    for (int v = 0; v < NV; v++)
+        for (int i = 0; i < Nc; i++) { o->R[v][i] = (o->R[v][i] + o->Rc[v][i])*o->ivR[i]; o->Rc[v][i] = 0; }
+#else
     for (int v = 0; v < NV; v++)
         for (int i = 0; i < Nc; i++) o->R[v][i] *= o->iv[i];
+#endif
 }
 
 /* Local time step at CFL 1 for each real cell c (iv_c != 0):
@@ -422,23 +482,24 @@ static void flux(hcfd_oracle* o) {
  * cell->face table (src/Mesh.cpp:88-117). */
 static void local_dt(hcfd_oracle* o) {
     const int Nc = o->Nc, Nf = o->Nf;
-    const double gmo = o->gma - 1;
-    double* lam = o->dtloc;
-    memset(lam, 0, sizeof(double)*Nc);
+    const real gma = RL(o->gma);
+    const real gmo = gma - 1;
+    real* lam = o->dtloc;
+    memset(lam, 0, sizeof(real)*Nc);
     for (int f = 0; f < Nf; f++) {
         int C2[2] = { o->fc_con[2*f], o->fc_con[2*f+1] };
         for (int s = 0; s < 2; s++) {
             int c = C2[s];
             if (o->iv[c] == 0.0) continue;
-            double ir = 1.0/o->U[0][c];
-            double u = o->U[1][c]*ir, v = o->U[2][c]*ir;
-            double p = gmo*(o->U[3][c] - 0.5*(o->U[1][c]*u + o->U[2][c]*v));
-            double a = sqrt(o->gma*p*ir);
-            double un = u*o->nf[2*f] + v*o->nf[2*f+1];
-            lam[c] += (fabs(un) + a)*o->Af[f];
+            real ir = RL(1.0)/o->U[0][c];
+            real u = o->U[1][c]*ir, v = o->U[2][c]*ir;
+            real p = gmo*(o->U[3][c] - RL(0.5)*(o->U[1][c]*u + o->U[2][c]*v));
+            real a = RSQRT(gma*p*ir);
+            real un = u*o->nfR[2*f] + v*o->nfR[2*f+1];
+            lam[c] += (fabs(un) + a)*o->AfR[f];
         }
     }
-    for (int i = 0; i < Nc; i++) lam[i] = (o->iv[i] != 0.0) ? 1.0/(o->iv[i]*lam[i]) : 0.0;
+    for (int i = 0; i < Nc; i++) lam[i] = (o->iv[i] != 0.0) ? RL(1.0)/(o->ivR[i]*lam[i]) : RL(0.0);
 }
 
 int hcfd_oracle_phase(hcfd_oracle* o, int which, double dt) {
@@ -449,9 +510,9 @@ int hcfd_oracle_phase(hcfd_oracle* o, int which, double dt) {
     case 3: flux(o); break;
     case 4:
         for (int v = 0; v < NV; v++)
-            for (int i = 0; i < o->Nc; i++) o->U[v][i] += dt*o->R[v][i];   /* Euler.cpp:107-113 */
+            for (int i = 0; i < o->Nc; i++) o->U[v][i] += RL(dt)*o->R[v][i];   /* Euler.cpp:107-113 */
         break;
-    case 5: for (int v = 0; v < NV; v++) memset(o->R[v], 0, sizeof(double)*o->Nc); break;
+    case 5: for (int v = 0; v < NV; v++) memset(o->R[v], 0, sizeof(real)*o->Nc); break;
     case 6: update_bc_cells(o); break;
     default: return -1;
     }
@@ -468,7 +529,7 @@ int hcfd_oracle_step(hcfd_oracle* o, int mode, double dt_or_cfl, double* dt_used
         for (int i = 0; i < Nc; i++) if (o->iv[i] != 0.0 && o->dtloc[i] < mn) mn = o->dtloc[i];
         dt = dt_or_cfl*mn;
         if (mode == HCFD_OR_LOCAL_CFL)
-            for (int i = 0; i < Nc; i++) o->dtloc[i] *= dt_or_cfl;
+            for (int i = 0; i < Nc; i++) o->dtloc[i] *= RL(dt_or_cfl);
     }
     gradient(o);
     o->nsteps++;
@@ -477,7 +538,7 @@ int hcfd_oracle_step(hcfd_oracle* o, int mode, double dt_or_cfl, double* dt_used
     flux(o);
     if (res_l2) {
         double s = 0.0;
-        for (int i = 0; i < Nc; i++) if (o->iv[i] != 0.0) s += o->R[0][i]*o->R[0][i];
+        for (int i = 0; i < Nc; i++) if (o->iv[i] != 0.0) s += (double) o->R[0][i]*(double) o->R[0][i];
         *res_l2 = sqrt(s/o->nreal);
     }
     if (mode == HCFD_OR_LOCAL_CFL) {
@@ -485,9 +546,9 @@ int hcfd_oracle_step(hcfd_oracle* o, int mode, double dt_or_cfl, double* dt_used
             for (int i = 0; i < Nc; i++) o->U[v][i] += o->dtloc[i]*o->R[v][i];
     } else {
         for (int v = 0; v < NV; v++)
-            for (int i = 0; i < Nc; i++) o->U[v][i] += dt*o->R[v][i];
+            for (int i = 0; i < Nc; i++) o->U[v][i] += RL(dt)*o->R[v][i];
     }
-    for (int v = 0; v < NV; v++) memset(o->R[v], 0, sizeof(double)*Nc);
+    for (int v = 0; v < NV; v++) memset(o->R[v], 0, sizeof(real)*Nc);
     update_bc_cells(o);
     if (dt_used) *dt_used = dt;
     return 0;
@@ -501,38 +562,42 @@ static void prims(hcfd_oracle* o) {
         if (v == ND+1) continue;
         for (int i = 0; i < Nc; i++) o->Q[v][i] = o->U[v][i]/o->U[0][i];
     }
-    double gmo = o->gma-1;
+    real gmo = RL(o->gma)-1;
     for (int i = 0; i < Nc; i++) {
-        double u[ND];
+        real u[ND];
         for (int d = 0; d < ND; d++) u[d] = o->Q[d+1][i];
-        o->Q[ND+1][i] = gmo * (o->U[ND+1][i] - 0.5*o->Q[0][i]*dot2(u,u));
+        o->Q[ND+1][i] = gmo * (o->U[ND+1][i] - RL(0.5)*o->Q[0][i]*dot2r(u,u));
     }
 }
+
+static void widen(double* out, const real* in, size_t n) { for (size_t k = 0; k < n; k++) out[k] = in[k]; }
+static void narrow(real* out, const double* in, size_t n) { for (size_t k = 0; k < n; k++) out[k] = RL(in[k]); }
 
 int hcfd_oracle_get(hcfd_oracle* o, int which, double* out) {
     const int Nc = o->Nc;
     switch (which) {
-    case HCFD_OR_U: for (int v = 0; v < NV; v++) memcpy(out + (size_t)v*Nc, o->U[v], sizeof(double)*Nc); break;
-    case HCFD_OR_Q: prims(o); for (int v = 0; v < NV; v++) memcpy(out + (size_t)v*Nc, o->Q[v], sizeof(double)*Nc); break;
-    case HCFD_OR_PHI: for (int v = 0; v < NV; v++) memcpy(out + (size_t)v*Nc, o->phi[v], sizeof(double)*Nc); break;
-    case HCFD_OR_R: for (int v = 0; v < NV; v++) memcpy(out + (size_t)v*Nc, o->R[v], sizeof(double)*Nc); break;
-    case HCFD_OR_G: for (int v = 0; v < NV; v++) memcpy(out + (size_t)v*2*Nc, o->G[v], sizeof(double)*2*Nc); break;
-    case HCFD_OR_DTLOC: local_dt(o); memcpy(out, o->dtloc, sizeof(double)*Nc); break;
+    case HCFD_OR_U: for (int v = 0; v < NV; v++) widen(out + (size_t)v*Nc, o->U[v], Nc); break;
+    case HCFD_OR_Q: prims(o); for (int v = 0; v < NV; v++) widen(out + (size_t)v*Nc, o->Q[v], Nc); break;
+    case HCFD_OR_PHI: for (int v = 0; v < NV; v++) widen(out + (size_t)v*Nc, o->phi[v], Nc); break;
+    case HCFD_OR_R: for (int v = 0; v < NV; v++) widen(out + (size_t)v*Nc, o->R[v], Nc); break;
+    case HCFD_OR_G: for (int v = 0; v < NV; v++) widen(out + (size_t)v*2*Nc, o->G[v], (size_t)2*Nc); break;
+    case HCFD_OR_DTLOC: local_dt(o); widen(out, o->dtloc, Nc); break;
     case HCFD_OR_IV: memcpy(out, o->iv, sizeof(double)*Nc); break;
     default: return -1;
     }
     return 0;
 }
 
+/* Replaces the state (rounded to the step's arithmetic). */
 int hcfd_oracle_set_U(hcfd_oracle* o, const double* u) {
-    for (int v = 0; v < NV; v++) memcpy(o->U[v], u + (size_t)v*o->Nc, sizeof(double)*o->Nc);
+    for (int v = 0; v < NV; v++) narrow(o->U[v], u + (size_t)v*o->Nc, o->Nc);
     return 0;
 }
 
 /* Replaces the limiter values (used by the next steps only while the limiter is frozen; an
  * unfrozen step recomputes them). */
 int hcfd_oracle_set_phi(hcfd_oracle* o, const double* phi) {
-    for (int v = 0; v < NV; v++) memcpy(o->phi[v], phi + (size_t)v*o->Nc, sizeof(double)*o->Nc);
+    for (int v = 0; v < NV; v++) narrow(o->phi[v], phi + (size_t)v*o->Nc, o->Nc);
     return 0;
 }
 

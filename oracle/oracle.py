@@ -22,6 +22,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libhcfd_oracle.so")
+ORACLE32_SO = os.path.join(HERE, "_build", "libhcfd_oracle32.so")
 REF_SO = os.path.join(HERE, "_ref", "libhcfd_ref.so")
 # where the reference sources lie when they are present (the Makefile's REF default)
 REF_DIR = os.environ.get("HCFD_REFERENCE", "/root/reference")
@@ -110,13 +111,15 @@ class Oracle:
     """The C restatement of the reference's Base solver (hcfd_oracle.c)."""
 
     _lib = None
+    _fp32 = False
 
     @classmethod
     def lib(cls):
         if cls._lib is None:
-            if not os.path.exists(ORACLE_SO):
-                raise RuntimeError(f"oracle library missing: {ORACLE_SO} (run make -C oracle)")
-            L = ct.CDLL(ORACLE_SO)
+            so = ORACLE32_SO if cls._fp32 else ORACLE_SO
+            if not os.path.exists(so):
+                raise RuntimeError(f"oracle library missing: {so} (run make -C oracle)")
+            L = ct.CDLL(so)
             L.hcfd_oracle_create.restype = ct.c_void_p
             L.hcfd_oracle_create.argtypes = [ct.c_int] * 5 + [_ip, _ip, _dp, _ip, _ip, _ip, _ip, ct.c_double]
             L.hcfd_oracle_free.argtypes = [ct.c_void_p]
@@ -218,6 +221,17 @@ class Oracle:
         self.lib().hcfd_oracle_domain(self.h, _d(rf), _d(nf), _d(Af), _d(If), _d(xc), _d(iv))
         return dict(rf=rf.reshape(Nf, 2, 2), nf=nf.reshape(Nf, 2), Af=Af, If=If,
                     xc=xc.reshape(Nc, 2), iv=iv)
+
+
+class Oracle32(Oracle):
+    """The same restatement built with float step arithmetic (HCFD_ORACLE_FP32): geometry in
+    double rounded once, state, gradients, limiter and fluxes in IEEE float, each cell's
+    residual summed with a compensated two-sum, dt minima and norms in double.  The CPU
+    counterpart of the library's FP32 path, which differs from it by the hardware's approximate
+    divisions and square roots (a few units in the last place per operation)."""
+
+    _lib = None
+    _fp32 = True
 
 
 class RefSolver:

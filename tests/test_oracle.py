@@ -353,3 +353,51 @@ def test_oracle_matches_reference_with_wall_and_subsonic_inlet(tmp_path, types):
     r.steps(30, 2e-3)
     assert np.isfinite(o.U()).all()
     assert np.array_equal(o.U(), r.U())
+
+
+def test_fp32_oracle_follows_fp64_at_float_rounding():
+    """The float build of the restatement (Oracle32, the CPU counterpart of the library's FP32
+    path) against the double one on a generated wedge: within float rounding after one step
+    and within 1e-5 over 50 steps, before the limiter's switching amplifies the difference."""
+    m = H.Mesh.wedge(61, 31, theta_deg=12.0, seed=1234, numbering=H.NUMBER_RANDOM)
+    bcmap, qbc, q = H.wedge_case(2.8)
+    a, b = O.Oracle(m.arrays()), O.Oracle32(m.arrays())
+    for o in (a, b):
+        o.gather_bcs(bcmap, qbc)
+        o.initialise(q)
+    assert np.max(O.rel_linf(b.U(), a.U())) <= 2.0 ** -24          # the initial state, rounded once
+    a.step(O.GLOBAL_CFL, 0.5)
+    b.step(O.GLOBAL_CFL, 0.5)
+    assert np.max(O.rel_linf(b.U(), a.U())) <= 3e-7
+    for _ in range(49):
+        a.step(O.GLOBAL_CFL, 0.5)
+        b.step(O.GLOBAL_CFL, 0.5)
+    assert np.max(O.rel_linf(b.U(), a.U())) <= 1e-5
+
+
+def test_handoff_at_the_freeze_leaves_an_fp32_steady_state_floor():
+    """FP64 to the freeze at step 100, then FP32 from the FP64 state and limiter values (the
+    handoff), against FP64 continuing, both to convergence (61 x 31 wedge, BJ, global CFL 0.5):
+    the handoff removes the O(1) difference of an FP32 solve that freezes its own limiter
+    values (0.58 here) but leaves the FP32 steady state's own error, about 1.3e-4 in L-inf
+    and 3e-5 in L2 (the FP32 residual stalls near 6e-5)."""
+    m = H.Mesh.wedge(61, 31, theta_deg=12.0, seed=1234, numbering=H.NUMBER_RANDOM)
+    bcmap, qbc, q = H.wedge_case(2.8)
+    a, b, c = O.Oracle(m.arrays()), O.Oracle32(m.arrays()), O.Oracle32(m.arrays())
+    for o in (a, b, c):
+        o.gather_bcs(bcmap, qbc)
+        o.initialise(q)
+        o.set_freeze(100)
+    for k in range(1, 4001):
+        ra = a.step(O.GLOBAL_CFL, 0.5)[1]
+        b.step(O.GLOBAL_CFL, 0.5)
+        c.step(O.GLOBAL_CFL, 0.5)
+        if k == 100:
+            b.set_U(a.U())
+            b.set_phi(a.get(O.F_PHI))
+    assert ra < 1e-6                                               # FP64 converged (from 2.7)
+    U64 = a.U()
+    handed, own = np.max(O.rel_linf(b.U(), U64)), np.max(O.rel_linf(c.U(), U64))
+    l2 = np.max(np.sqrt(((b.U() - U64) ** 2).mean(axis=1)) / np.sqrt((U64 ** 2).mean(axis=1)))
+    assert own > 0.1
+    assert handed < 3e-4 and handed < own / 1000 and l2 < 1e-4
