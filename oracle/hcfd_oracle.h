@@ -10,6 +10,10 @@
  * The features the reference does not have (global CFL dt, local time stepping, the
  * Venkatakrishnan limiter, the L2 density residual and the wall pressure coefficient) are
  * defined here; their parity with the GPU solver is pinned only by this restatement.
+ *
+ * Built with HCFD_ORACLE_FP32 the same source steps in float (geometry rounded once from
+ * double, compensated per-cell residual sums): the CPU counterpart of the FP32 path.  The
+ * interface below is the same in both builds (doubles in and out).
  */
 #ifndef HCFD_ORACLE_H
 #define HCFD_ORACLE_H

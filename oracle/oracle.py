@@ -5,6 +5,7 @@ only as the checker or as the timed CPU baseline.  The product (cfd_optimisation
 never imports it.
 
 * ``Oracle``      — the C restatement in hcfd_oracle.c (built into _build/).
+* ``Oracle32``    — the same source built with float step arithmetic (HCFD_ORACLE_FP32).
 * ``RefSolver``   — the reference's own layouts, compiled unchanged into _ref/ by the
                     Makefile here (present only where the reference sources were
                     available at build time; the built library travels with the repo).
