@@ -61,7 +61,13 @@ struct hcfd_oracle {
 static inline double dot2(const double* a, const double* b) { return a[0]*b[0] + a[1]*b[1]; }
 static inline real dot2r(const real* a, const real* b) { return a[0]*b[0] + a[1]*b[1]; }
 
-#ifdef HCFD_ORACLE_FP32
+/* HCFD_ORACLE_NOCOMP (float build only): plain float sums instead of two-sums, to measure what
+ * the compensation buys. */
+#if defined(HCFD_ORACLE_FP32) && !defined(HCFD_ORACLE_NOCOMP)
+#define HCFD_ORACLE_COMP 1
+#endif
+
+#ifdef HCFD_ORACLE_COMP
 /* s + c += x (Knuth's two-sum); the library's FP32 path accumulates each cell's residual so. */
 static inline void two_sum(real* s, real* c, real x) {
     real t = *s + x;
@@ -456,7 +462,7 @@ static void flux(hcfd_oracle* o) {
         for (int v = 0; v < NV; v++) UfR[v] = UR[v] + phiR[v]*dot2r(GR[v], rR);
         rusanov(UfL, UfR, &o->nfR[2*f], RL(o->gma), Ff);
         for (int v = 0; v < NV; v++) {
-#ifdef HCFD_ORACLE_FP32
+#ifdef HCFD_ORACLE_COMP
             two_sum(&o->R[v][CL], &o->Rc[v][CL], -(Af*Ff[v]));
             two_sum(&o->R[v][CR], &o->Rc[v][CR], Af*Ff[v]);
 #else
@@ -465,12 +471,12 @@ static void flux(hcfd_oracle* o) {
 #endif
         }
     }
-#ifdef HCFD_ORACLE_FP32
+#ifdef HCFD_ORACLE_COMP
     for (int v = 0; v < NV; v++)
         for (int i = 0; i < Nc; i++) { o->R[v][i] = (o->R[v][i] + o->Rc[v][i])*o->ivR[i]; o->Rc[v][i] = 0; }
 #else
     for (int v = 0; v < NV; v++)
-        for (int i = 0; i < Nc; i++) o->R[v][i] *= o->iv[i];
+        for (int i = 0; i < Nc; i++) o->R[v][i] *= o->ivR[i];
 #endif
 }
 

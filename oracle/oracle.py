@@ -5,7 +5,8 @@ only as the checker or as the timed CPU baseline.  The product (cfd_optimisation
 never imports it.
 
 * ``Oracle``      — the C restatement in hcfd_oracle.c (built into _build/).
-* ``Oracle32``    — the same source built with float step arithmetic (HCFD_ORACLE_FP32).
+* ``Oracle32``    — the same source built with float step arithmetic (HCFD_ORACLE_FP32);
+                    ``Oracle32NoComp`` without its compensated sums.
 * ``RefSolver``   — the reference's own layouts, compiled unchanged into _ref/ by the
                     Makefile here (present only where the reference sources were
                     available at build time; the built library travels with the repo).
@@ -24,6 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libhcfd_oracle.so")
 ORACLE32_SO = os.path.join(HERE, "_build", "libhcfd_oracle32.so")
+ORACLE32NC_SO = os.path.join(HERE, "_build", "libhcfd_oracle32nc.so")
 REF_SO = os.path.join(HERE, "_ref", "libhcfd_ref.so")
 # where the reference sources lie when they are present (the Makefile's REF default)
 REF_DIR = os.environ.get("HCFD_REFERENCE", "/root/reference")
@@ -112,12 +114,12 @@ class Oracle:
     """The C restatement of the reference's Base solver (hcfd_oracle.c)."""
 
     _lib = None
-    _fp32 = False
+    _so = "double"
 
     @classmethod
     def lib(cls):
         if cls._lib is None:
-            so = ORACLE32_SO if cls._fp32 else ORACLE_SO
+            so = {"double": ORACLE_SO, "float": ORACLE32_SO, "float-nocomp": ORACLE32NC_SO}[cls._so]
             if not os.path.exists(so):
                 raise RuntimeError(f"oracle library missing: {so} (run make -C oracle)")
             L = ct.CDLL(so)
@@ -232,7 +234,14 @@ class Oracle32(Oracle):
     divisions and square roots (a few units in the last place per operation)."""
 
     _lib = None
-    _fp32 = True
+    _so = "float"
+
+
+class Oracle32NoComp(Oracle):
+    """Oracle32 with plain float sums in place of the compensated ones (HCFD_ORACLE_NOCOMP)."""
+
+    _lib = None
+    _so = "float-nocomp"
 
 
 class RefSolver:
