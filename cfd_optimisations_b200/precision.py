@@ -25,12 +25,14 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
+import tempfile
 import time
 
 import numpy as np
 
 from . import (FP32, FP64, GLOBAL_CFL, LIMITER_BJ, LIMITER_VENKAT, LOCAL_CFL, NUMBER_RANDOM, Mesh, Solver,
-               wedge_case)
+               convert_checkpoint, wedge_case)
 from .native import ENONFINITE, HcfdError
 
 LOWER_WALL = 2   # colour of the lower wall (the ramp) in the generated wedge
@@ -168,9 +170,6 @@ def handoff(mesh: Mesh, mach: float, cfl: float, steps: int, every: int, freeze:
     solve's limiter values.  Beside it an FP32 solve that ran from the start freezes its own.
     From step `freeze` on, the three step side by side and the two FP32 solves' errors against
     FP64 are recorded as _lockstep records them."""
-    import os
-    import tempfile
-    from . import convert_checkpoint
     fp64 = _solver(mesh, FP64, limiter, K, freeze, mach)
     own = _solver(mesh, FP32, limiter, K, freeze, mach)
     fp64.step(freeze, mode, cfl)
