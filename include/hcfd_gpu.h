@@ -93,13 +93,15 @@ int  hcfd_mesh_load(const char* path, hcfd_mesh** out);
 /* Writes the .hmsh layout of interface/Mesh.py:441-463 (header, names, coltag, coloff,
  * nodes, fn_con, fc_con, cn_off, cn_con, cc_off, cc_con, c_ctypes). */
 int  hcfd_mesh_write(const hcfd_mesh* m, const char* path);
-/* Fills *v with pointers into m (valid until m is freed or renumbered). */
+/* Fills *v with pointers into m (valid until m is freed or renumbered): the arrays the
+ * reference's Mesh exposes as public members (includes/Mesh.hpp:4-13). */
 int  hcfd_mesh_view_of(const hcfd_mesh* m, hcfd_mesh_view* v);
 /* The CSR cell->face table of Mesh::compute_cf_con (src/Mesh.cpp:88-117): the faces of
  * cell c, in increasing face index, are cf_con[cf_off[c] .. cf_off[c+1]). */
 int  hcfd_mesh_cf(const hcfd_mesh* m, const int** cf_off, const int** cf_con);
 /* Physical name k (the reference's Mesh::pnames, src/Mesh.cpp:70-86) or NULL. */
 const char* hcfd_mesh_pname(const hcfd_mesh* m, int k);
+/* Replaces Mesh::~Mesh (src/Mesh.cpp:54-68). */
 void hcfd_mesh_free(hcfd_mesh* m);
 
 /* Supersonic-wedge generator (the mesh family of the reference's wedge.hmsh, produced
@@ -211,18 +213,21 @@ void hcfd_snapshot_free(hcfd_snapshot* t);
 int  hcfd_gpu_checkpoint(hcfd_solver* s, const char* path);
 int  hcfd_gpu_restore(hcfd_solver* s, const char* path);
 int  hcfd_checkpoint_info(const char* path, int* Nc, int* precision, long long* steps, int* has_limiter);
-/* Waits for the handle's stream; returns HCFD_ENONFINITE if a step produced a NaN/Inf. */
+/* Waits for the handle's stream; returns HCFD_ENONFINITE if a step produced a NaN/Inf (no
+ * reference counterpart: the reference steps synchronously and never checks for NaN). */
 int  hcfd_gpu_sync(hcfd_solver* s);
-/* Statistics of the steps taken so far (waits for the stream). */
+/* Statistics of the steps taken so far (waits for the stream; no reference counterpart:
+ * the reference computes no residual). */
 int  hcfd_gpu_stats(hcfd_solver* s, hcfd_step_stats* stats);
 /* Wall pressure coefficient (p_CL - p_inf) / (0.5 rho_inf |u_inf|^2) on the faces of one
  * colour, in face order; *n gets the face count.  No reference counterpart. */
 int  hcfd_gpu_wall_cp(hcfd_solver* s, int colour, double rho_inf, double p_inf, double speed_inf,
                       double* out, int* n);
 /* Mesh facts as the solver sees them: Nc, Nf, number of real (non-ghost) cells, the
- * face slots per cell of the step kernels. */
+ * face slots per cell of the step kernels (no reference counterpart). */
 int  hcfd_gpu_info(hcfd_solver* s, int* Nc, int* Nf, int* Nreal, int* slots);
-/* Per-kernel timing with CUDA events on the handle's stream.  enable = N > 0 starts
+/* Per-kernel timing with CUDA events on the handle's stream (the reference times only whole
+ * runs, with clock(), src/Test.cpp:72-74).  enable = N > 0 starts
  * recording the two step kernels' launches of every N-th step (N > 1 keeps the events'
  * own cost out of most steps); 0 stops.  hcfd_gpu_profile_read returns the summed
  * milliseconds and launch counts of the recorded launches since enabling. */
@@ -233,12 +238,15 @@ int  hcfd_gpu_profile_read(hcfd_solver* s, double* ms_pass1, long long* n_pass1,
  * CUDA events recorded on the handle's stream before the first and after the last launch.
  * No reference counterpart (the reference times whole runs with clock(), src/Test.cpp:72-74). */
 int  hcfd_gpu_step_timed(hcfd_solver* s, int nsteps, int time_mode, double dt_or_cfl, double* ms);
-/* Number of kernel launches one step issues (the two passes). */
+/* Number of kernel launches one step issues (the two passes; no reference counterpart). */
 int  hcfd_gpu_launches_per_step(hcfd_solver* s);
+/* Replaces the Euler destructor (src/Base/Euler.cpp:27-40) and those of the objects
+ * hcfd_gpu_create stands in for: frees the handle's device memory, stream and graphs. */
 void hcfd_gpu_destroy(hcfd_solver* s);
 
 /* Page-locks a caller-owned host range (cudaHostRegister) so that hcfd_gpu_upload and
- * hcfd_gpu_download from and to it run as direct DMA; hcfd_host_unpin releases it. */
+ * hcfd_gpu_download from and to it run as direct DMA; hcfd_host_unpin releases it (no
+ * reference counterpart). */
 int  hcfd_host_pin(void* p, size_t bytes);
 int  hcfd_host_unpin(void* p);
 
@@ -374,12 +382,16 @@ int  hcfd_write_hsln(const char* path, int nvars, const char* const* varnames, i
 
 /* Makes `device` the calling thread's current CUDA device for the handles it creates
  * afterwards (one process per GPU; a handle stays on the device it was created on).
- * *count, if non-NULL, gets the number of visible devices. */
+ * *count, if non-NULL, gets the number of visible devices.  No reference counterpart (the
+ * reference is a single-threaded CPU program), nor for hcfd_device_sync. */
 int  hcfd_set_device(int device, int* count);
 /* Waits for all work on the current device (cudaDeviceSynchronize). */
 int  hcfd_device_sync(void);
 
 /* ---- errors ------------------------------------------------------------------------- */
+/* Text of the calling thread's last failure.  No reference counterpart: the reference
+ * reports no errors (no return codes or exceptions; fopen and fread results unchecked,
+ * src/Mesh.cpp:9-45, src/Writer.cpp:25). */
 const char* hcfd_last_error(void);
 
 #ifdef __cplusplus
