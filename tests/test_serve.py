@@ -165,3 +165,18 @@ def test_serve_devices_runs_one_server_per_device():
     for (dev, arena), part in zip(sorted(made, key=lambda m: m[0]), parts):
         assert sorted(arena.admitted) == sorted(r.rid for r in part)     # each device served its share
     assert all(x.steps == 300 for x in res)                               # 10**(-0.02 n) <= 1e-6 at n = 300
+
+
+def test_sequential_service_and_step_models():
+    """The FP64 sequential baseline's estimators: queueing in arrival order, and the affine
+    step-cost fit recovering a known fixed cost and per-cell cost."""
+    reqs = [serve.Request(i, t, 0, 0, 2.0, 10.0, i) for i, t in enumerate((0.0, 0.5, 10.0))]
+    steps = {0: 10, 1: 10, 2: 20}
+    # 0.1 s per step: request 0 runs 0..1, request 1 waits until 1 and runs to 2, request 2 runs 10..12
+    span, lat = serve.sequential_service(reqs, steps, lambda t: 0.1)
+    assert span == pytest.approx(12.0) and lat == pytest.approx([1.0, 1.5, 2.0])
+    x = np.array([5e3, 2e4, 8e4, 3e5, 1e6, 2e6])
+    a, b = serve.affine_step_model(x, 2e-5 + 1.1e-10 * x)
+    assert a == pytest.approx(2e-5, rel=1e-6) and b == pytest.approx(1.1e-10, rel=1e-6)
+    a, b = serve.affine_step_model(x, 1.1e-10 * x - 1e-6)              # a negative fixed cost is clamped
+    assert a == 0.0 and b > 0
