@@ -24,9 +24,11 @@ The baseline runs each request alone through the plain FP64 solver (Solver, one 
 time, the same stopping rule checked every `chunk` steps).  Timing it over the whole stream
 would take hours; it is run on `baseline-sample` requests (every k-th request in arrival
 order) and the stream's sequential service time is estimated from them per cell-step, stated
-in the output (the headline ratio; conservative, since small meshes cost more per cell-step
-than the large ones that dominate the rate).  A second estimate fits a step cost a + b *
-triangles to the sample.  The same sample gives the served results' errors against FP64.
+in the output (the headline ratio).  One rate per cell-step is exact when a step's cost is
+proportional to its cells; with a fixed cost per step as well, it is right only when the
+sample's cell-step-weighted mean size matches the stream's.  A second estimate therefore fits
+a step cost a + b * triangles to the sample and applies it request by request.  The same
+sample gives the served results' errors against FP64.
 """
 from __future__ import annotations
 
@@ -366,9 +368,7 @@ def main():
         errs64.append(float((np.abs(U64b - U64).max(axis=1) / den).max()))
     per_cell_step = sum(s for _, s, _ in base) / sum(r.triangles * i["steps"] for r, _, i in base)
     # sequential service of the whole stream, each request's time estimated from its cell-steps
-    # (steps per request as served).  One rate per cell-step, dominated by the large sampled
-    # meshes, undercounts the launch-bound small ones: the conservative estimate, and the
-    # headline ratio.
+    # (steps per request as served); the headline ratio
     steps_by_rid = {x.rid: x.steps for x in res}
     t_free, lat_b = sequential_service(reqs, steps_by_rid, lambda tri: per_cell_step * tri)
     out["fp64_sequential"] = dict(sample=len(base), sample_device_s=sum(s for _, s, _ in base),
@@ -377,7 +377,8 @@ def main():
                                   note="device time of the sampled requests, extrapolated per cell-step to the "
                                        "stream (steps per request as served)")
     out["speedup_solves_per_s"] = out["served"]["solves_per_s"] / out["fp64_sequential"]["solves_per_s"]
-    # the same with a step cost a + b * triangles fitted to the sample (fixed cost per step)
+    # the same with a step cost a + b * triangles fitted to the sample: the fixed cost per step
+    # charged request by request, whatever the sample's mean size
     a0, b0 = affine_step_model([r.triangles for r, _, _ in base], [s / i["steps"] for r, s, i in base])
     t_aff, lat_aff = sequential_service(reqs, steps_by_rid, lambda tri: a0 + b0 * tri)
     out["fp64_sequential_affine"] = dict(s_per_step_fixed=a0, s_per_cell_step=b0, estimated_makespan_s=t_aff,
