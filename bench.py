@@ -257,6 +257,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-variants", action="store_true", help="skip the random-numbering and FP32 lines")
     ap.add_argument("--mesh", default=f"{NX}x{NY}", help="node grid NXxNY (profiling of smaller cases)")
+    ap.add_argument("--kernel", choices=["tiled", "cell"], default="tiled",
+                    help="step kernel family (the per-cell gather kernels are the other fusion split)")
     ap.add_argument("--profile-only", action="store_true",
                     help="warm-up and timed steps only (no end-to-end, variants or CPU legs): for ncu")
     args = ap.parse_args()
@@ -274,7 +276,8 @@ def main():
     H.set_device(local)
     mesh = make_mesh(H.NUMBER_RCM)
     bcmap, qbc, q = H.wedge_case(MACH)
-    s = H.Solver(mesh, limiter=H.LIMITER_VENKAT, venkat_K=VENKAT_K, precision=H.FP64)
+    kernel = H.KERNEL_CELL if args.kernel == "cell" else H.KERNEL_TILED
+    s = H.Solver(mesh, limiter=H.LIMITER_VENKAT, venkat_K=VENKAT_K, precision=H.FP64, kernel=kernel)
     s.gather_bcs(bcmap, qbc)
     s.initialise(q)
     ntri = s.Nreal
@@ -307,13 +310,14 @@ def main():
     peak, peak_kind = peaks()
     achieved = b / (t * 1e-3) / 1e9
     step_achieved = (b1 + b2) / (ms_max / args.steps * 1e-3) / 1e9
-    traffic = traffic_from_profiles(dom, f"fp64_rcm_{NX}x{NY}")
+    traffic = traffic_from_profiles(dom, f"fp64_rcm_{NX}x{NY}" + ("_cell" if args.kernel == "cell" else ""))
 
     line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD + ", RCM numbering", "cells": Nc, "real_cells": ntri, "faces": Nf,
+            "config": {"workload": WORKLOAD + ", RCM numbering" + (", per-cell kernels" if args.kernel == "cell" else ""),
+                       "cells": Nc, "real_cells": ntri, "faces": Nf,
                        "parallelism": f"{world} replica(s), one per GPU, no collective",
                        "l2": "per-step working set > 1.6 GB, far above the 126 MB L2; no flush"},
             "gpu_launches": s.launches_per_step() * args.steps,
