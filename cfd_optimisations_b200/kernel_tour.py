@@ -9,9 +9,10 @@ through set-up (geometry, renumbering, face records), initialise and boundary ce
 global and local CFL mode, an asynchronous snapshot, download, upload, the wall pressure
 coefficient and a checkpoint / restore.  Arena: `instances` wedges of 10,000 to 60,000
 triangles admitted to one FP32 arena (admission kernels), stepped, polled, fetched,
-checkpointed, restored and released.  The cells and faces of every stepped case exceed the
-126 MB L2, so the DRAM figures of the step kernels are those of a full-size run.  Prints one
-JSON line with the cells touched and the steps taken.
+checkpointed, restored and released.  An FP64 step on the single mesh moves 0.45 GB, well
+above the 126 MB L2, so its kernels' DRAM figures are those of a full-size run; the FP32 and
+arena passes move 0.1-0.2 GB each, about the L2's size, so part of their traffic can hit in L2.
+Prints one JSON line with the cells touched and the steps taken.
 """
 from __future__ import annotations
 
