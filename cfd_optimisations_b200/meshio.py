@@ -346,6 +346,14 @@ def main(argv=None):
     p = sp.add_parser("checkcell", help="one cell's type, nodes, neighbours and centre")
     p.add_argument("meshin")
     p.add_argument("cell", type=int)
+    p = sp.add_parser("wedge", help="generate a triangulated supersonic wedge -> .hmsh")
+    p.add_argument("nx", type=int)
+    p.add_argument("ny", type=int)
+    p.add_argument("meshout")
+    p.add_argument("--theta", type=float, default=15.0, help="ramp angle, degrees")
+    p.add_argument("--jitter", type=float, default=0.15, help="interior node jitter, fraction of the spacing")
+    p.add_argument("--seed", type=int, default=1234)
+    p.add_argument("--numbering", choices=["natural", "random", "rcm", "morton"], default="random")
     a = ap.parse_args(argv)
     if a.cmd == "import":
         import_msh(a.meshin, a.meshout)
@@ -353,6 +361,13 @@ def main(argv=None):
         export(a.mesh, a.solnin, a.solnout)
     elif a.cmd == "bexport":
         batch_export(a.mesh, a.solnin_pattern, a.solnout_pattern, a.Wnone)
+    elif a.cmd == "wedge":
+        import cfd_optimisations_b200 as H
+        num = {"natural": H.NUMBER_NATURAL, "random": H.NUMBER_RANDOM, "rcm": H.NUMBER_RCM,
+               "morton": H.NUMBER_MORTON}[a.numbering]
+        m = H.Mesh.wedge(a.nx, a.ny, theta_deg=a.theta, jitter=a.jitter, seed=a.seed, numbering=num)
+        m.write(a.meshout)
+        print(f"{a.meshout}: {m.Nc} cells, {m.Nf} faces")
     else:
         print(check_cell(a.meshin, a.cell))
 

@@ -241,3 +241,16 @@ def test_generated_wedge_matches_the_reference_importer_up_to_numbering(golden):
     cells_b, faces_b = _canonical(ref)
     assert cells_a == cells_b
     assert faces_a == faces_b and len(faces_a) == m["Nf"]
+
+
+def test_wedge_command_writes_the_generated_mesh(tmp_path, capsys):
+    """`python -m cfd_optimisations_b200.meshio wedge` writes the generator's mesh, readable by
+    the library's checked reader and identical to the one the Python API builds."""
+    out = tmp_path / "w.hmsh"
+    meshio.main(["wedge", "41", "21", str(out), "--theta", "12", "--seed", "3", "--numbering", "rcm"])
+    assert "1720 cells" in capsys.readouterr().out                    # 1,600 triangles + 120 ghosts
+    a = H.Mesh(str(out)).arrays()
+    b = H.Mesh.wedge(41, 21, theta_deg=12.0, seed=3, numbering=H.NUMBER_RCM).arrays()
+    assert a["Nc"] == 2 * 40 * 20 + 2 * 40 + 2 * 20 and a["Nf"] == b["Nf"]
+    for k in ("nodes", "fc_con", "fn_con", "cn_off", "cn_con", "coloff"):
+        assert np.array_equal(a[k], b[k]), k
