@@ -16,6 +16,9 @@ Export writes an UnstructuredGrid .vtu with inline base64 binary arrays: points 
 (triangle, quad and line cells with VTK types 5, 9, 3), and one cell array per solution variable,
 the velocity components combined into one 3-component vector "Velocity", as the reference's
 exporter names them.
+
+`wedge NX NY OUT` writes the library's generated supersonic wedge (hcfd_mesh_generate_wedge)
+as .hmsh, the mesh family of the workloads, without gmsh.
 """
 from __future__ import annotations
 
