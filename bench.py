@@ -1,10 +1,11 @@
 #!/usr/bin/env python
-"""Benchmark of the per-step residual-and-update loop on the large supersonic wedge.
+"""Benchmark of the per-step residual-and-update loop on the large supersonic wedge, with the
+batched and served legs.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (one "step" = one solver time step over the whole mesh): the triangulated wedge
-of 2001 x 1001 nodes (4,000,000 triangles + 6,000 ghost cells, 6,003,000 faces), x in
+Headline workload (one "step" = one solver time step over the whole mesh): the triangulated
+wedge of 2001 x 1001 nodes (4,000,000 triangles + 6,000 ghost cells, 6,003,000 faces), x in
 [0, 3], top wall y = 1.5, ramp of 15 degrees from x = 0.5, interior nodes jittered by
 U(+-0.15) of the local spacing, seeded diagonals; freestream rho 1.4, p 1, u 2.5 (M 2.5);
 Venkatakrishnan limiter K = 5; global CFL 0.5; FP64; cells RCM-renumbered.  Synthetic,
@@ -13,14 +14,26 @@ generated in-process from fixed seeds.
 Metric: cell-updates/s = real cells x steps / time.  The per-step working set (~1.7 GB)
 is far larger than the 126 MB L2, so no flush is needed between steps.
 
-Under torchrun (N > 1) every rank runs its own replica of the workload on its own GPU
-(the path does not shard: replicas only, no collective on the data path); the reported
-time is the maximum over ranks and the value is the total over ranks.
+Legs beside the headline (rank 0, one GPU):
+* variants: random cell numbering; FP32; and the reference's own arithmetic on the same mesh
+  (Barth-Jespersen, fixed dt), the configuration the reference arm can run;
+* cpu_baseline: the reference's fastest valid CPU layout on the host cores, same mesh, same
+  fixed-dt configuration;
+* batched: 512 wedges of 2,000-200,000 triangles in one FP32 arena, 2000 steps each, against
+  the plain FP64 solver looped over them (cfd_optimisations_b200/batched.py);
+* served: the first requests of the seeded 10,000-request stream (Poisson arrivals at 100/s),
+  continuous batching into one FP32 arena, against the plain sequential FP64 loop run on every
+  one of the same requests (cfd_optimisations_b200/serve.py).
 
-`--impl reference` times the reference's own CPU solver (compiled unchanged into
-oracle/_ref): its fastest layout that matches its Base layout to 1e-12 after one step
-(VEC, AVX2 build), fixed dt, Barth-Jespersen limiter (the reference has no
-Venkatakrishnan limiter and no CFL control), one independent instance per host core.
+Under torchrun (N > 1) every rank runs its own replica of the headline workload on its own GPU
+(the path does not shard: replicas only, no collective on the data path); the reported time
+is the maximum over ranks and the value is the total over ranks.
+
+`--impl reference` times the reference's own CPU solver (compiled unchanged into oracle/_ref):
+its fastest layout that matches its Base layout to 1e-12 after one step (VEC, AVX2 build), on
+the same mesh written by the oracle's generator (the product library is not loaded), fixed dt
+(the reference has no CFL control) and the Barth-Jespersen limiter (it has no Venkatakrishnan
+limiter), one independent instance per host core.
 """
 from __future__ import annotations
 
@@ -41,8 +54,35 @@ sys.path.insert(0, ROOT)
 NX, NY = 2001, 1001
 THETA, MACH, SEED = 15.0, 2.5, 1234
 VENKAT_K, CFL = 5.0, 0.5
-WORKLOAD = (f"supersonic wedge {NX}x{NY} nodes ({2 * (NX - 1) * (NY - 1):,} triangles), M{MACH} "
-            f"{THETA:g}deg, Venkatakrishnan K{VENKAT_K:g}, global CFL {CFL}, FP64")
+REF_MAX_STEPS, REF_MAX_WARMUP = 60, 5      # keeps the reference arm within about two minutes
+
+
+def workload() -> str:
+    return (f"supersonic wedge {NX}x{NY} nodes ({2 * (NX - 1) * (NY - 1):,} triangles), M{MACH} "
+            f"{THETA:g}deg, Venkatakrishnan K{VENKAT_K:g}, global CFL {CFL}, FP64, RCM numbering")
+
+
+def freestream_case(mach: float = MACH, rho: float = 1.4, p: float = 1.0, gma: float = 1.4):
+    """BC map and states of the wedge case (the same values as the package's wedge_case):
+    colour tags 1 upper / 2 lower SYMMETRY, 3 inlet SUPINLET, 4 outlet SUPOUTLET
+    (src/Test.cpp:64); uniform freestream (rho, M a, 0, p)."""
+    a = (gma * p / rho) ** 0.5
+    q = np.array([rho, mach * a, 0.0, p])
+    return np.array([0, 0, 0, 2, 4], dtype=np.int32), np.tile(q, (4, 1)), q
+
+
+def reference_dt() -> float:
+    """The fixed dt of the reference's configuration: half the CFL-0.5 step of a cell of the
+    x-spacing in the freestream (stable over the benchmark's steps; the reference has no CFL
+    control, so both arms use this one number)."""
+    _, _, q = freestream_case()
+    a = (1.4 * q[3] / q[0]) ** 0.5
+    return CFL * 0.5 * (3.0 / (NX - 1)) / (q[1] + a)
+
+
+def reference_workload() -> str:
+    return (f"supersonic wedge {NX}x{NY} nodes ({2 * (NX - 1) * (NY - 1):,} triangles), M{MACH} "
+            f"{THETA:g}deg, Barth-Jespersen, fixed dt {reference_dt():.6e}, FP64, RCM numbering")
 
 
 def peaks():
@@ -158,58 +198,49 @@ def traffic_from_profiles(kernel: str, workload_key: str):
     return None if e is None else float(e)
 
 
-def cpu_reference(mesh, steps: int, dt: float, threads: int | None = None):
+def cpu_reference(steps: int, warmup: int, threads: int | None = None):
     """The reference solver's VEC layout (AVX2 build, compiled unchanged) over `threads`
-    independent instances; returns (cell-updates/s, threads, seconds)."""
+    independent instances of the wedge (written by the oracle's generator, not the product
+    library), Barth-Jespersen, fixed dt reference_dt(); returns (cell-updates/s, threads,
+    seconds, sample text) or None when the reference library was not built."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    import cfd_optimisations_b200 as H
     if not O.RefSolver.available():
         return None
     nthreads = threads or os.cpu_count() or 1
-    try:  # about 1.7 GB per instance of this mesh
+    try:  # about 1.8 GB per instance of this mesh
         with open("/proc/meminfo") as fh:
             avail = next(int(l.split()[1]) for l in fh if l.startswith("MemAvailable")) * 1024
-        nthreads = max(1, min(nthreads, int(0.6 * avail / 1.8e9)))
+        nthreads = max(1, min(nthreads, int(0.6 * avail / (1.8e9 * NX * NY / 2.003e6))))
     except (OSError, StopIteration):
         pass
-    bcmap, qbc, q = H.wedge_case(MACH)
+    bcmap, qbc, q = freestream_case()
+    dt = reference_dt()
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "wedge.hmsh")
-        mesh.write(path)
-        secs = O.RefSolver.bench("VEC", path, bcmap, qbc, q, nthreads, 1, steps, dt)
+        O.wedge_hmsh(path, NX, NY, theta_deg=THETA, jitter=0.15, seed=SEED, numbering=O.NUMBER_RCM)
+        secs = O.RefSolver.bench("VEC", path, bcmap, qbc, q, nthreads, warmup, steps, dt)
     ntri = 2 * (NX - 1) * (NY - 1)
-    return ntri * steps * nthreads / secs, nthreads, secs
+    sample = (f"reference VEC layout (AVX2 build, compiled unchanged), {nthreads} independent instances x {steps} "
+              f"steps of the {NX}x{NY} wedge after {warmup} warm-up steps; Barth-Jespersen, fixed dt {dt:.6e} "
+              f"(the reference has no Venkatakrishnan limiter or CFL control); mesh from the oracle's generator")
+    return ntri * steps * nthreads / secs, nthreads, secs, sample
 
 
 def run_reference_arm(args):
-    rank, world, local, dist = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0, None
-    if rank != 0:
+    """Rank 0 alone times the reference (the other ranks exit without work)."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    import cfd_optimisations_b200 as H
-    try:
-        mesh = make_mesh(H.NUMBER_RCM)
-    except Exception as e:  # no native library: the mesh generator is part of it
-        print(json.dumps({"impl": "reference", "unavailable": f"mesh generator unavailable: {e}"}))
-        return 0
-    # dt: the global CFL-0.5 dt of the freestream state (constant while the flow is uniform).
-    bcmap, qbc, q = H.wedge_case(MACH)
-    a = (1.4 * q[3] / q[0]) ** 0.5
-    dx = 3.0 / (NX - 1)
-    dt = CFL * 0.5 * dx / (q[1] + a)
-    steps = max(1, min(args.steps, 2))
-    r = cpu_reference(mesh, steps, dt)
+    steps, warm = max(1, min(args.steps, REF_MAX_STEPS)), max(1, min(args.warmup, REF_MAX_WARMUP))
+    r = cpu_reference(steps, warm)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhcfd_ref.so not built"}))
         return 0
-    value, threads, secs = r
-    sample = (f"reference VEC layout (AVX2 build, compiled unchanged), {threads} independent instances x "
-              f"{steps} steps of the {NX}x{NY} wedge after 1 warm-up step; fixed dt {dt:.3e}; "
-              f"Barth-Jespersen (the reference has no Venkatakrishnan limiter or CFL control)")
+    value, threads, secs, sample = r
     line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus,
-            "steps": steps, "warmup": 1, "ms_per_step": secs / steps * 1e3, "higher_is_better": True,
+            "steps": steps, "warmup": warm, "ms_per_step": secs / steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD + ", RCM numbering", "parallelism": f"{threads} CPU replicas"},
+            "config": {"workload": reference_workload(), "parallelism": f"{threads} CPU replicas, one per host thread"},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
                              "sample": sample},
@@ -247,26 +278,44 @@ def e2e_run(H, mesh, steps: int):
     return t, nbytes / steps, (nbytes + stats_bytes * steps) / steps
 
 
+def timed_variant(H, mesh, ntri, Nc, Nf, peak, steps, warmup, limiter, prec, mode, value):
+    """Device time of `steps` steps of one more configuration on the same kind of mesh."""
+    v = H.Solver(mesh, limiter=limiter, venkat_K=VENKAT_K, precision=prec)
+    bcmap, qbc, q = H.wedge_case(MACH)
+    v.gather_bcs(bcmap, qbc)
+    v.initialise(q)
+    v.step(warmup, mode, value)
+    mv = v.step_timed(steps, mode, value)
+    ww = 8 if prec == H.FP64 else 4
+    balg = 30 * ww * Nc + 2 * (8 + 7 * ww) * Nf
+    return {"cell_updates_per_s": ntri * steps / (mv * 1e-3), "ms_per_step": mv / steps, "steps": steps,
+            "step_achieved_GBs": balg / (mv / steps * 1e-3) / 1e9,
+            "step_frac": balg / (mv / steps * 1e-3) / 1e9 / peak}
+
+
 def main():
-    global NX, NY, WORKLOAD
+    global NX, NY
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--no-variants", action="store_true", help="skip the random-numbering and FP32 lines")
+    ap.add_argument("--no-variants", action="store_true", help="skip the random-numbering, FP32 and BJ lines")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched leg")
+    ap.add_argument("--no-served", action="store_true", help="skip the served leg")
+    ap.add_argument("--batched-instances", type=int, default=512)
+    ap.add_argument("--batched-steps", type=int, default=2000)
+    ap.add_argument("--served-requests", type=int, default=100)
     ap.add_argument("--mesh", default=f"{NX}x{NY}", help="node grid NXxNY (profiling of smaller cases)")
     ap.add_argument("--kernel", choices=["tiled", "cell"], default="tiled",
                     help="step kernel family (the per-cell gather kernels are the other fusion split)")
     ap.add_argument("--profile-only", action="store_true",
-                    help="warm-up and timed steps only (no end-to-end, variants or CPU legs): for ncu")
+                    help="warm-up and timed steps only (no end-to-end, variants, CPU, batched or served legs): for ncu")
     args = ap.parse_args()
     NX, NY = (int(x) for x in args.mesh.lower().split("x"))
-    WORKLOAD = (f"supersonic wedge {NX}x{NY} nodes ({2 * (NX - 1) * (NY - 1):,} triangles), M{MACH} "
-                f"{THETA:g}deg, Venkatakrishnan K{VENKAT_K:g}, global CFL {CFL}, FP64")
     if args.profile_only:
-        args.no_cpu = args.no_variants = True
+        args.no_cpu = args.no_variants = args.no_batched = args.no_served = True
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -316,7 +365,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD + ", RCM numbering" + (", per-cell kernels" if args.kernel == "cell" else ""),
+            "config": {"workload": workload() + (", per-cell kernels" if args.kernel == "cell" else ""),
                        "cells": Nc, "real_cells": ntri, "faces": Nf,
                        "parallelism": f"{world} replica(s), one per GPU, no collective",
                        "l2": "per-step working set > 1.6 GB, far above the 126 MB L2; no flush"},
@@ -339,33 +388,49 @@ def main():
                        "how": "hcfd_gpu_upload of the pinned state, per step hcfd_gpu_step + stats read, "
                               "hcfd_gpu_download of the primitive state into pinned memory; host wall clock"}
 
+    single = rank == 0 and world == 1
     if not args.no_variants and rank == 0:
-        var = {}
-        for name, num, prec in (("fp64_random", H.NUMBER_RANDOM, H.FP64), ("fp32_rcm", H.NUMBER_RCM, H.FP32)):
-            m2 = mesh if num == H.NUMBER_RCM else make_mesh(num)
-            v = H.Solver(m2, limiter=H.LIMITER_VENKAT, venkat_K=VENKAT_K, precision=prec)
-            v.gather_bcs(bcmap, qbc)
-            v.initialise(q)
-            v.step(args.warmup, H.GLOBAL_CFL, CFL)
-            k = min(args.steps, 200)
-            mv = v.step_timed(k, H.GLOBAL_CFL, CFL)
-            ww = 8 if prec == H.FP64 else 4
-            balg = 30 * ww * Nc + 2 * (8 + 7 * ww) * Nf
-            var[name] = {"cell_updates_per_s": ntri * k / (mv * 1e-3), "ms_per_step": mv / k,
-                         "step_achieved_GBs": balg / (mv / k * 1e-3) / 1e9,
-                         "step_frac": balg / (mv / k * 1e-3) / 1e9 / peak}
-            del v
+        k = min(args.steps, 200)
+        var = {"fp64_random": timed_variant(H, make_mesh(H.NUMBER_RANDOM), ntri, Nc, Nf, peak, k, args.warmup,
+                                            H.LIMITER_VENKAT, H.FP64, H.GLOBAL_CFL, CFL),
+               "fp32_rcm": timed_variant(H, mesh, ntri, Nc, Nf, peak, k, args.warmup, H.LIMITER_VENKAT, H.FP32,
+                                         H.GLOBAL_CFL, CFL),
+               "fp64_bj_fixed_dt": timed_variant(H, mesh, ntri, Nc, Nf, peak, args.steps, args.warmup,
+                                                 H.LIMITER_BJ, H.FP64, H.FIXED_DT, reference_dt())}
+        var["fp64_bj_fixed_dt"]["workload"] = reference_workload()
         line["variants"] = var
 
-    if rank == 0 and world == 1 and not args.no_cpu:
-        dt_cpu = st["dt"]
-        r = cpu_reference(mesh, 2, dt_cpu)
+    if single and not args.no_cpu:
+        r = cpu_reference(max(1, min(args.steps, 2)), 1)
         if r is not None:
-            cv, threads, secs = r
+            cv, threads, secs, sample = r
             line["cpu_baseline"] = {"value": cv, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
-                                    "sample": f"reference VEC layout (AVX2 build, compiled unchanged), {threads} "
-                                              f"independent instances x 2 steps of this mesh (BJ limiter, fixed "
-                                              f"dt {dt_cpu:.3e}), {secs:.1f} s"}
+                                    "sample": sample}
+            if "variants" in line:
+                g = line["variants"]["fp64_bj_fixed_dt"]["cell_updates_per_s"]
+                line["same_config_as_reference"] = {
+                    "workload": reference_workload(), "gpu_cell_updates_per_s": g, "cpu_cell_updates_per_s": cv,
+                    "gpu_over_cpu": g / cv,
+                    "note": "the reference arm's own configuration (Barth-Jespersen, fixed dt) on the GPU, "
+                            "against the reference on the host cores in this run"}
+
+    if single and not args.no_batched:
+        from cfd_optimisations_b200 import batched
+        t0 = time.perf_counter()
+        b = batched.run(args.batched_instances, args.batched_steps, spread_every=4)
+        b["wall_s"] = time.perf_counter() - t0
+        line["batched"] = b
+
+    if single and not args.no_served:
+        from cfd_optimisations_b200 import serve
+        t0 = time.perf_counter()
+        sv = serve.run_prefix(args.served_requests)
+        sv["wall_s"] = time.perf_counter() - t0
+        per = sv.pop("per_request")
+        sv["per_request"] = {k: [p[k] for p in per] for k in ("triangles", "latency_s", "fp32_vs_fp64",
+                                                              "fp64_one_rounding_spread")}
+        line["served"] = sv
+
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -312,6 +312,13 @@ def set_device(device: int) -> int:
     return n.value
 
 
+def device_mem_info() -> tuple[int, int]:
+    """(free, total) bytes of device memory on the current device."""
+    f, t = ct.c_size_t(), ct.c_size_t()
+    _n.check(_n.lib().hcfd_device_mem_info(ct.byref(f), ct.byref(t)))
+    return f.value, t.value
+
+
 def device_sync() -> None:
     _n.check(_n.lib().hcfd_device_sync())
 

@@ -26,7 +26,7 @@ enum { LIM_BJ = 0, LIM_VENKAT = 1 };
 enum { TM_FIXED = 0, TM_GLOBAL = 1, TM_LOCAL = 2 };
 
 // Face record: unit normal (oriented out of CL), length, interpolation weight and the two
-// centre-to-face vectors (src/Base/Domain.hpp:15-20).  64 B in double, 32 B in float.
+// centre-to-face vectors (includes/Base/Domain.hpp:15-20).  64 B in double, 32 B in float.
 template <class T>
 struct alignas(8 * sizeof(T)) FaceGeo {
     T nx, ny, Af, If, rLx, rLy, rRx, rRy;

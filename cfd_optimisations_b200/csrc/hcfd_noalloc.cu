@@ -13,6 +13,9 @@
 #include "hcfd_internal.hpp"
 #include "hcfd_kernels.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -36,9 +39,43 @@ constexpr size_t kScratchBytes = kStats + 256;
 // memory: kernels get the device address taken by cudaGetSymbolAddress at set-up.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
+// The device address of the scratch belongs to a CUDA context: after cudaDeviceReset (or
+// any other end of the context) the device holds a new copy at a new address.  The address
+// is therefore cached per device together with the unique id of the context it was taken in
+// (cuCtxGetId, ids are never reused within a process) and looked up again when the current
+// context's id differs.  The two driver calls come through cudaGetDriverEntryPointByVersion,
+// so the library needs no link against libcuda.
 constexpr int kMaxDevices = 64;
-unsigned char* g_addr[kMaxDevices] = {nullptr};
+struct ScratchAddr {
+    unsigned long long ctx_id;   // 0: not looked up yet
+    unsigned char* addr;
+};
+ScratchAddr g_addr[kMaxDevices] = {};
 std::mutex g_addr_mu;
+PFN_cuCtxGetCurrent_v4000 g_ctx_current = nullptr;
+PFN_cuCtxGetId_v12000 g_ctx_id = nullptr;
+bool g_entry_points_tried = false;
+
+// Id of the calling thread's current context, 0 when there is none or it cannot be told.
+unsigned long long current_ctx_id() {
+    if (!g_entry_points_tried) {
+        g_entry_points_tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f);
+    }
+    if (!g_ctx_current || !g_ctx_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_current(&c) != CUDA_SUCCESS || !c || g_ctx_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // Clears what must start at zero (and the dt minimum at +inf) on every call.
 __global__ void noalloc_reset_kernel(unsigned long long* dtmin, unsigned int* counter, hcfd::StepStats* stats) {
@@ -63,16 +100,29 @@ void launch(const hcfd::StepArgs<double>& a, cudaStream_t st) {
 extern "C" int hcfd_step_noalloc(const hcfd_noalloc_mesh* m, const double* U_in, double* U_out, int time_mode,
                                  double dt_or_cfl, void* stream, double* dt_used, double* res_l2) {
     hcfd::clear_error();
-    if (!m || !U_in || !U_out || U_in == U_out || !m->slot || !m->geo || !m->iv)
-        return fail(HCFD_EINVAL, "step_noalloc: null or aliased argument");
+    if (!m || !U_in || !U_out || !m->slot || !m->geo || !m->iv)
+        return fail(HCFD_EINVAL, "step_noalloc: null argument");
     if (m->Nc <= 0 || m->Nc > HCFD_NOALLOC_MAX_CELLS)
         return fail(HCFD_EINVAL, "step_noalloc: Nc must be in 1.." + std::to_string(HCFD_NOALLOC_MAX_CELLS) +
                                      " (the size of the static scratch)");
+    {
+        // pass 2 writes U_out while other cells still read U_in: the ranges must be disjoint
+        const uintptr_t a0 = reinterpret_cast<uintptr_t>(U_in), b0 = reinterpret_cast<uintptr_t>(U_out);
+        const uintptr_t n = sizeof(double) * 4 * (uintptr_t) m->Nc;
+        if (a0 < b0 + n && b0 < a0 + n) return fail(HCFD_EINVAL, "step_noalloc: U_in and U_out overlap");
+    }
     if (m->Nf <= 0 || m->F_BC < 0 || m->F_BC > m->Nf || (m->slots != 3 && m->slots != 4 && m->slots != 8) ||
         m->nbc < 0 || m->nbc > hcfd::MAXBC || (m->nbc > 0 && (!m->bc_first || !m->bc_type || !m->bc_state)) ||
         !(m->gma > 1.0) || (m->limiter != HCFD_LIMITER_BJ && m->limiter != HCFD_LIMITER_VENKAT) ||
         time_mode < HCFD_FIXED_DT || time_mode > HCFD_GLOBAL_CFL || !std::isfinite(dt_or_cfl) || dt_or_cfl < 0)
         return fail(HCFD_EINVAL, "step_noalloc: bad argument");
+    // The boundary table must cover exactly the boundary faces F_BC..Nf-1, in order: a face
+    // outside it would be refreshed with another colour's type and state.
+    if (m->nbc == 0 ? m->F_BC != m->Nf : (m->bc_first[0] != m->F_BC || m->bc_first[m->nbc] != m->Nf))
+        return fail(HCFD_EINVAL, "step_noalloc: the boundary colours must cover faces F_BC..Nf-1");
+    for (int b = 0; b < m->nbc; b++)
+        if (m->bc_first[b + 1] < m->bc_first[b])
+            return fail(HCFD_EINVAL, "step_noalloc: bc_first must not decrease");
 
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -80,16 +130,21 @@ extern "C" int hcfd_step_noalloc(const hcfd_noalloc_mesh* m, const double* U_in,
     if (dev < 0 || dev >= kMaxDevices) return fail(HCFD_EINVAL, "step_noalloc: device index too large");
     unsigned char* base;
     {
-        // Once per device, with that device current: the device address of the scratch.
+        // Once per device and context, with that device current: the device address of the
+        // scratch.  Where the context id cannot be read, the address is looked up on every
+        // call (a host-side lookup; it allocates nothing).
         std::lock_guard<std::mutex> lk(g_addr_mu);
-        if (!g_addr[dev]) {
+        const unsigned long long id = current_ctx_id();
+        if (id == 0 || g_addr[dev].ctx_id != id) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p)
                 return fail(HCFD_ECUDA, std::string("step_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_addr[dev] = static_cast<unsigned char*>(p);
+            // the lookup makes the device's context current if none was: take its id now
+            g_addr[dev].ctx_id = current_ctx_id();
+            g_addr[dev].addr = static_cast<unsigned char*>(p);
         }
-        base = g_addr[dev];
+        base = g_addr[dev].addr;
     }
 
     hcfd::BCTable bc{};

@@ -970,6 +970,13 @@ int hcfd_device_sync(void) {
     return HCFD_OK;
 }
 
+int hcfd_device_mem_info(size_t* free_bytes, size_t* total_bytes) {
+    hcfd::clear_error();
+    if (!free_bytes || !total_bytes) return fail(HCFD_EINVAL, "device_mem_info: null argument");
+    CK(cudaMemGetInfo(free_bytes, total_bytes));
+    return HCFD_OK;
+}
+
 void hcfd_gpu_destroy(hcfd_solver* s) {
     if (!s) return;
     free_all(s);

@@ -132,6 +132,7 @@ _SIGS = {
     "hcfd_arena_destroy": (None, [ct.c_void_p]),
     "hcfd_set_device": (ct.c_int, [ct.c_int, _ip]),
     "hcfd_device_sync": (ct.c_int, []),
+    "hcfd_device_mem_info": (ct.c_int, [ct.POINTER(ct.c_size_t), ct.POINTER(ct.c_size_t)]),
     "hcfd_last_error": (ct.c_char_p, []),
 }
 

@@ -42,7 +42,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import FP32, FP64, GLOBAL_CFL, LIMITER_BJ, NUMBER_RANDOM, Mesh, Solver, wedge_case
+from . import FP32, FP64, GLOBAL_CFL, LIMITER_BJ, NUMBER_RANDOM, Mesh, Solver, device_mem_info, wedge_case
 from .native import ENONFINITE, HcfdError
 
 
@@ -289,6 +289,77 @@ def percentiles(x) -> dict:
     return dict(p50=float(np.percentile(x, 50)), p99=float(np.percentile(x, 99)), mean=float(x.mean()))
 
 
+def arena_budget(budget_gb: float) -> int:
+    """The HBM budget: `budget_gb` GB, capped at the device's free memory less 4 GB."""
+    free, _ = device_mem_info()
+    return int(min(budget_gb * 1e9, free - 4e9))
+
+
+def run_prefix(n: int = 100, rate: float = 100.0, seed: int = 7, orders: float = 6.0, max_steps: int = 20000,
+               chunk: int = 100, cfl: float = 0.5, budget_gb: float = 160.0, spread_every: int = 4,
+               workers: int = 8) -> dict:
+    """The first `n` requests of the seeded stream, served, against the plain sequential FP64
+    GPU loop run on every one of the same requests (nothing extrapolated).
+
+    Served: continuous batching into one FP32 arena (Server).  Sequential: each request alone
+    through the plain FP64 solver in arrival order, a request starting when it has arrived and
+    the previous one is done; its service time is the device time of its steps (CUDA events;
+    mesh construction and solver set-up are not charged to it, while the served latencies
+    include them).  Every request's FP32 result is compared with its FP64 result; every
+    `spread_every`-th request is also solved in FP64 from an initial density one rounding step
+    larger, the spread rounding alone produces in that solve."""
+    from . import autotune
+    from .arena import Arena
+    from .batched import accuracy_summary, rel_linf_max
+    reqs = request_stream(10000, rate, seed)[:n]
+    budget = arena_budget(budget_gb)
+    med = int(np.median([r.triangles for r in reqs]))
+    tile = autotune.best_arena_tile(med, FP32, LIMITER_BJ)
+    arena = Arena(budget, precision=FP32, limiter=LIMITER_BJ, time_mode=GLOBAL_CFL, tile=tile,
+                  max_instances=max(64, 2 * n))
+    srv = Server(arena, cfl, orders, max_steps, chunk, workers=workers, keep=lambda rid: True)
+    res = srv.run(reqs)
+    span = max(r.t_done for r in res)
+    del srv.arena, arena
+    dev_s, U64, info64 = {}, {}, {}
+    for r in reqs:
+        ms, info, U = solve_alone_fp64(r, cfl, orders, max_steps, chunk)
+        dev_s[r.rid], U64[r.rid], info64[r.rid] = ms / 1e3, U, info
+    t_free, lat_seq = 0.0, []
+    for r in reqs:
+        t_free = max(t_free, r.t_arrive) + dev_s[r.rid]
+        lat_seq.append(t_free - r.t_arrive)
+    by = {x.rid: x for x in res}
+    e32 = {r.rid: rel_linf_max(by[r.rid].U, U64[r.rid]) for r in reqs}
+    sub = [r for i, r in enumerate(reqs) if i % max(1, spread_every) == 0]
+    e64 = {}
+    for r in sub:
+        _, _, Up = solve_alone_fp64(r, cfl, orders, max_steps, chunk, rho_scale=1.0 + 2.0 ** -52)
+        e64[r.rid] = rel_linf_max(Up, U64[r.rid])
+    served = dict(precision="fp32-compensated", tile=tile, budget_bytes=budget, makespan_s=span,
+                  solves_per_s=n / span, latency_s=percentiles([x.latency for x in res]),
+                  queue_s=percentiles([x.t_admit - x.t_arrive for x in res]),
+                  converged=sum(x.converged for x in res), failed=sum(x.failed for x in res),
+                  steps=percentiles([x.steps for x in res]), device_busy_fraction=srv.busy_s / span,
+                  max_active=srv.max_active)
+    seq = dict(precision="fp64", makespan_s=t_free, solves_per_s=n / t_free, latency_s=percentiles(lat_seq),
+               device_s=sum(dev_s.values()), converged=sum(i["why"] == "converged" for i in info64.values()),
+               steps=percentiles([i["steps"] for i in info64.values()]),
+               how="every request alone through the plain FP64 solver in arrival order; device time of its steps")
+    return dict(workload=dict(requests=n, of_stream=10000, rate_per_s=rate, seed=seed,
+                              triangles="lognormal median 5e4 sigma 1.0 clipped [5e3, 2e6]",
+                              triangles_total=int(sum(r.triangles for r in reqs)), mach="U[1.8,4.0]",
+                              theta_deg="U[5,15]", stop=f"{orders} orders or {max_steps} steps", chunk=chunk,
+                              limiter="barth-jespersen", cfl=cfl),
+                served=served, fp64_sequential=seq, speedup_solves_per_s=served["solves_per_s"] / seq["solves_per_s"],
+                accuracy=accuracy_summary([e32[r.rid] for r in sub], [e64[r.rid] for r in sub]),
+                fp32_vs_fp64_rel_linf=dict(n=n, median=float(np.median(list(e32.values()))),
+                                           max=float(max(e32.values()))),
+                per_request=[dict(rid=r.rid, triangles=r.triangles, latency_s=by[r.rid].latency,
+                                  steps=by[r.rid].steps, fp32_vs_fp64=e32[r.rid],
+                                  fp64_one_rounding_spread=e64.get(r.rid)) for r in reqs])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=10000)
@@ -309,11 +380,9 @@ def main():
 
     from . import autotune
     from .arena import Arena
-    import torch  # noqa: F401  (device memory query only)
 
     reqs = request_stream(a.requests, a.rate, a.seed)
-    free, total = torch.cuda.mem_get_info()
-    budget = int(min(a.budget_gb * 1e9, free - 4e9))
+    budget = arena_budget(a.budget_gb)
     med = int(np.median([r.triangles for r in reqs]))
     tile = a.tile or autotune.best_arena_tile(med, FP32, LIMITER_BJ)
     k = max(1, len(reqs) // max(1, a.baseline_sample))

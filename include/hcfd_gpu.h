@@ -346,10 +346,13 @@ typedef struct hcfd_noalloc_mesh {
                                the other cell}; unused slots {-1, -1}; a ghost cell's first slot
                                is unused.  Each cell's faces in increasing face index.          */
     const double* geo;      /* device, Nf x 8: nx, ny, length, If, rLx, rLy, rRx, rRy (the
-                               reference's Domain arrays, src/Base/Domain.hpp:15-24)             */
+                               layout of the reference's Domain face arrays,
+                               includes/Base/Domain.hpp:15-24)                                    */
     const double* iv;       /* device, Nc: 1/area, 0 for ghost cells                               */
     int nbc;                /* boundary colours (0..16)                                           */
-    const int* bc_first;    /* host, nbc + 1: first face of each boundary colour, then Nf         */
+    const int* bc_first;    /* host, nbc + 1: first face of each boundary colour, then Nf;
+                               non-decreasing, bc_first[0] = F_BC, bc_first[nbc] = Nf
+                               (nbc = 0 requires F_BC = Nf)                                       */
     const int* bc_type;     /* host, nbc: enum hcfd_bctype                                        */
     const double* bc_state; /* host, nbc x 4: primitive (rho, u, v, p)                            */
     double gma;
@@ -357,15 +360,19 @@ typedef struct hcfd_noalloc_mesh {
     double venkat_K;
 } hcfd_noalloc_mesh;
 
-/* One step (HCFD_FIXED_DT or HCFD_GLOBAL_CFL) from U_in to U_out, both caller-owned device
- * buffers of 4 Nc doubles that must not overlap, laid out as two planes of pairs: plane 0
- * holds (rho, rho u) of cells 0..Nc-1, plane 1 (at offset 2 Nc) holds (rho v, E).  Work is
+/* New entry point, no reference counterpart.  One step (HCFD_FIXED_DT or HCFD_GLOBAL_CFL)
+ * from U_in to U_out, both caller-owned device buffers of 4 Nc doubles whose address ranges
+ * must not overlap (HCFD_EINVAL otherwise), laid out as two planes of pairs: plane 0 holds
+ * (rho, rho u) of cells 0..Nc-1, plane 1 (at offset 2 Nc) holds (rho v, E).  Work is
  * enqueued on `stream` (a cudaStream_t, NULL for the default stream).  When dt_used or
- * res_l2 is non-NULL the call waits for the stream and reports the step's dt and L2 density
- * residual.  Allocates nothing: no cudaMalloc, cudaFree or allocating library call.
- * The first call on each device looks up the device address of the static scratch; make
- * that first call before any stream capture.  All calls share the one scratch array, which
- * keeps the last call's contents: calls that overlap on the GPU (other streams, other
+ * res_l2 is non-NULL the call waits for the stream, reports the step's dt and L2 density
+ * residual, and returns HCFD_ENONFINITE if the step produced a NaN or Inf; with both NULL
+ * it returns without waiting and nothing checks the new state for NaN or Inf.  Allocates
+ * nothing: no cudaMalloc, cudaFree or allocating library call.
+ * The first call on each device (and again the first call after the device's context was
+ * replaced, e.g. by cudaDeviceReset) looks up the device address of the static scratch;
+ * make that first call before any stream capture.  All calls share the one scratch array,
+ * which keeps the last call's contents: calls that overlap on the GPU (other streams, other
  * threads) race and must be serialised by the caller. */
 int  hcfd_step_noalloc(const hcfd_noalloc_mesh* mesh, const double* U_in, double* U_out, int time_mode,
                        double dt_or_cfl, void* stream, double* dt_used, double* res_l2);
@@ -387,6 +394,9 @@ int  hcfd_write_hsln(const char* path, int nvars, const char* const* varnames, i
 int  hcfd_set_device(int device, int* count);
 /* Waits for all work on the current device (cudaDeviceSynchronize). */
 int  hcfd_device_sync(void);
+/* Free and total device memory of the current device in bytes (cudaMemGetInfo), for sizing
+ * an arena's HBM budget.  No reference counterpart. */
+int  hcfd_device_mem_info(size_t* free_bytes, size_t* total_bytes);
 
 /* ---- errors ------------------------------------------------------------------------- */
 /* Text of the calling thread's last failure.  No reference counterpart: the reference

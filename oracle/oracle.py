@@ -10,6 +10,8 @@ never imports it.
 * ``RefSolver``   — the reference's own layouts, compiled unchanged into _ref/ by the
                     Makefile here (present only where the reference sources were
                     available at build time; the built library travels with the repo).
+* ``wedge_hmsh``  — writes the triangulated wedge as a .hmsh file (hcfd_oracle_mesh.c), the
+                    input of the timed reference arm, without the product library.
 * ``read_hmsh`` / ``read_hsln`` — independent numpy readers of the two file formats,
   following src/Mesh.cpp:7-54 and src/Writer.cpp:22-39 of the reference.
 """
@@ -26,6 +28,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libhcfd_oracle.so")
 ORACLE32_SO = os.path.join(HERE, "_build", "libhcfd_oracle32.so")
 ORACLE32NC_SO = os.path.join(HERE, "_build", "libhcfd_oracle32nc.so")
+MESH_SO = os.path.join(HERE, "_build", "libhcfd_oracle_mesh.so")
 REF_SO = os.path.join(HERE, "_ref", "libhcfd_ref.so")
 # where the reference sources lie when they are present (the Makefile's REF default)
 REF_DIR = os.environ.get("HCFD_REFERENCE", "/root/reference")
@@ -53,6 +56,28 @@ def build(ref: bool = True) -> None:
     """Builds the oracle (and, when the reference sources exist, the reference library)."""
     targets = ["oracle"] + (["ref"] if ref and os.path.isdir(os.path.join(REF_DIR, "src")) else [])
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+NUMBER_NATURAL, NUMBER_RANDOM, NUMBER_RCM, NUMBER_MORTON = range(4)
+_mesh_lib = None
+
+
+def wedge_hmsh(path: str, nx: int, ny: int, theta_deg: float = 15.0, jitter: float = 0.15, seed: int = 1234,
+               numbering: int = NUMBER_RANDOM, length: float = 3.0, height: float = 1.5, x_ramp: float = 0.5) -> None:
+    """Writes the triangulated supersonic wedge to `path` (.hmsh), the same file the library's
+    generator writes for the same arguments (hcfd_oracle_mesh.c)."""
+    global _mesh_lib
+    if _mesh_lib is None:
+        if not os.path.exists(MESH_SO):
+            raise RuntimeError(f"oracle mesh library missing: {MESH_SO} (run make -C oracle)")
+        L = ct.CDLL(MESH_SO)
+        L.hcfd_oracle_wedge_hmsh.argtypes = [ct.c_int, ct.c_int] + [ct.c_double] * 5 + [ct.c_ulonglong, ct.c_int,
+                                                                                       ct.c_char_p]
+        _mesh_lib = L
+    rc = _mesh_lib.hcfd_oracle_wedge_hmsh(nx, ny, length, height, x_ramp, theta_deg, jitter, seed, numbering,
+                                          os.fsencode(path))
+    if rc != 0:
+        raise ValueError(f"wedge_hmsh: {'bad arguments or an inverted triangle' if rc == -1 else 'I/O error'}")
 
 
 def read_hmsh(path: str) -> dict:

@@ -49,3 +49,25 @@ def test_traffic_of_the_committed_profile():
 def test_aggregate_is_whole_job_throughput():
     # 4 ranks, 1e9 units each, slowest rank 500 ms
     assert bench.aggregate(1e9, 4, 500.0) == 8e9
+
+
+def test_reference_arm_runs_the_reference_without_the_product_library():
+    """bench.py --impl reference on a small wedge: one JSON line from the reference compiled
+    unchanged, K timed steps after W warm-up steps, and no product library in the process."""
+    import json
+    import subprocess
+    import sys
+    import oracle as O
+    if not O.RefSolver.available():
+        import pytest
+        pytest.skip("the reference library was not built here")
+    code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--mesh', '41x21', '--steps', '3', "
+            "'--warmup', '4']; import bench; bench.main(); maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'product_loaded': 'libhcfd_gpu' in maps, 'ref_loaded': 'libhcfd_ref' in maps}))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=bench.ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    line, probe = (json.loads(x) for x in out.stdout.strip().splitlines()[-2:])
+    assert probe == {"product_loaded": False, "ref_loaded": True}
+    assert line["impl"] == "reference" and line["steps"] == 3 and line["warmup"] == 4
+    assert "Barth-Jespersen, fixed dt" in line["config"]["workload"]
+    assert line["value"] > 0 and line["e2e"]["h2d_bytes_per_step"] == 0

@@ -6,8 +6,9 @@ cudaFree can synchronise the device).  They keep the inputs and outputs in their
 buffers and the step takes its scratch from a static device array of the library.  Here the
 caller's buffers are allocated by torch, on the caller's side; the entry point is called
 through the C ABI twice in a row and each result is checked against the existing entry
-point (hcfd_gpu_step) on the same mesh and state, at the one-step tolerance of the parity
-tests.  The file is named so that pytest collects it last.
+point (hcfd_gpu_step) on the same mesh and state, and against the oracle, at the one-step
+tolerance of the parity tests.  The argument checks run on the host and need no GPU.  The
+file is named so that pytest collects it last.
 """
 import ctypes as ct
 
@@ -17,8 +18,6 @@ import pytest
 import cfd_optimisations_b200 as H
 from cfd_optimisations_b200 import native as N
 import oracle as O
-
-pytestmark = pytest.mark.gpu
 
 ONE_STEP = 1e-12
 
@@ -58,20 +57,24 @@ def _unplanes(p, Nc):
     return np.stack([p0[:, 0], p0[:, 1], p1[:, 0], p1[:, 1]])
 
 
-def test_noalloc_step_matches_solver_step_twice():
+def _noalloc_case(mesh, bcmap, qbc, q, limiter, K, time_mode, value):
+    """Two steps through hcfd_step_noalloc from the initial state, each checked against the
+    existing entry point (hcfd_gpu_step, per-cell kernels in the caller's numbering) and
+    against the oracle, at the one-step tolerance."""
     torch = pytest.importorskip("torch")
-    mesh = H.Mesh.wedge(81, 41, theta_deg=15.0, seed=17, numbering=H.NUMBER_RANDOM)
-    bcmap, qbc, q = H.wedge_case(2.5)
-
-    # the existing entry point
-    s = H.Solver(mesh, kernel=H.KERNEL_CELL, keep_numbering=True)
+    s = H.Solver(mesh, kernel=H.KERNEL_CELL, keep_numbering=True, limiter=limiter, venkat_K=K)
     s.gather_bcs(bcmap, qbc)
     s.initialise(q)
     U0 = s.U()
+    o = O.Oracle(mesh.arrays())
+    o.gather_bcs(bcmap, qbc)
+    o.initialise(q)
+    o.set_limiter(O.VENKAT if limiter == H.LIMITER_VENKAT else O.BJ, K)
     ref = []
     for _ in range(2):
-        st = s.step(1, H.GLOBAL_CFL, 0.5)
-        ref.append((s.U(), st["dt"], st["res_l2"]))
+        st = s.step(1, time_mode, value)
+        dt_o, res_o = o.step(time_mode, value)
+        ref.append((s.U(), st["dt"], st["res_l2"], o.U(), dt_o, res_o))
 
     # the caller's own device buffers
     a, F_BC, W, slot, geo, iv = _tables(mesh)
@@ -86,23 +89,65 @@ def test_noalloc_step_matches_solver_step_twice():
 
     ncol, nbc = a["Ncol"], a["NBCcol"]
     bc_first = np.ascontiguousarray(a["coloff"][ncol - nbc:ncol + 1], dtype=np.int32)
-    bc_type = np.ascontiguousarray(bcmap[a["coltag"][ncol - nbc:ncol]], dtype=np.int32)
+    bc_type = np.ascontiguousarray(np.asarray(bcmap)[a["coltag"][ncol - nbc:ncol]], dtype=np.int32)
     bc_state = np.ascontiguousarray(qbc, dtype=np.float64).reshape(-1)
     m = N.NoallocMesh(Nc, Nf, F_BC, W, d_slot.data_ptr(), d_geo.data_ptr(), d_iv.data_ptr(),
                       nbc, bc_first.ctypes.data_as(N._ip), bc_type.ctypes.data_as(N._ip),
-                      bc_state.ctypes.data_as(N._dp), 1.4, H.LIMITER_BJ, 5.0)
+                      bc_state.ctypes.data_as(N._dp), 1.4, limiter, K)
     lib = N.lib()
     for i in range(2):
         dt, res = ct.c_double(), ct.c_double()
         rc = lib.hcfd_step_noalloc(ct.byref(m), d_U[i % 2].data_ptr(), d_U[(i + 1) % 2].data_ptr(),
-                                   H.GLOBAL_CFL, 0.5, None, ct.byref(dt), ct.byref(res))
+                                   time_mode, value, None, ct.byref(dt), ct.byref(res))
         N.check(rc)
         torch.cuda.synchronize()
         U = _unplanes(d_U[(i + 1) % 2].cpu().numpy(), Nc)
-        U_ref, dt_ref, res_ref = ref[i]
+        U_ref, dt_ref, res_ref, U_o, dt_o, res_o = ref[i]
         assert np.all(O.rel_linf(U, U_ref) <= ONE_STEP), O.rel_linf(U, U_ref)
-        assert abs(dt.value - dt_ref) <= 1e-13 * dt_ref
-        assert abs(res.value - res_ref) <= 1e-10 * res_ref
+        assert np.all(O.rel_linf(U, U_o) <= ONE_STEP), O.rel_linf(U, U_o)
+        for d in (dt_ref, dt_o):
+            assert abs(dt.value - d) <= 1e-13 * d
+        for r in (res_ref, res_o):
+            assert abs(res.value - r) <= 1e-10 * r
+    return W
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("limiter,K", [(H.LIMITER_BJ, 0.0), (H.LIMITER_VENKAT, 5.0)])
+@pytest.mark.parametrize("time_mode,value", [(H.FIXED_DT, 2e-4), (H.GLOBAL_CFL, 0.5)])
+def test_noalloc_step_matches_solver_step_twice(limiter, K, time_mode, value):
+    mesh = H.Mesh.wedge(81, 41, theta_deg=15.0, seed=17, numbering=H.NUMBER_RANDOM)
+    bcmap, qbc, q = H.wedge_case(2.5)
+    assert _noalloc_case(mesh, bcmap, qbc, q, limiter, K, time_mode, value) == 3
+
+
+@pytest.mark.gpu
+def test_noalloc_step_on_a_mixed_quad_triangle_mesh(tmp_path):
+    """A gmsh-imported mesh of quadrangles and triangles: four face slots per cell."""
+    from test_meshio import write_msh
+    from cfd_optimisations_b200 import meshio
+    write_msh(tmp_path / "r.msh", nx=41, ny=21)
+    meshio.import_msh(str(tmp_path / "r.msh"), str(tmp_path / "r.hmsh"))
+    mesh = H.Mesh(str(tmp_path / "r.hmsh"))
+    bcmap = [H.SYMMETRY, H.SYMMETRY, H.SUPOUTLET, H.SYMMETRY, H.SUPINLET]
+    q = (1.4, 2.2, 0.35, 1.0)
+    assert _noalloc_case(mesh, bcmap, [q] * 4, q, H.LIMITER_BJ, 0.0, H.GLOBAL_CFL, 0.5) == 4
+
+
+def _bad_mesh(**kw):
+    f = dict(Nc=100, Nf=160, F_BC=150, slots=3, nbc=2, bc_first=[150, 155, 160])
+    f.update(kw)
+    first = np.ascontiguousarray(f["bc_first"], dtype=np.int32)
+    types = np.zeros(max(f["nbc"], 1), dtype=np.int32)
+    state = np.ones(4 * max(f["nbc"], 1))
+    m = N.NoallocMesh(f["Nc"], f["Nf"], f["F_BC"], f["slots"], 16, 16, 16, f["nbc"], first.ctypes.data_as(N._ip),
+                      types.ctypes.data_as(N._ip), state.ctypes.data_as(N._dp), 1.4, 0, 5.0)
+    return m, (first, types, state)
+
+
+def _call(m, U_in=4096, U_out=65536):
+    return N.lib().hcfd_step_noalloc(ct.byref(m), ct.c_void_p(U_in), ct.c_void_p(U_out), H.FIXED_DT, 1e-3,
+                                     None, None, None)
 
 
 def test_noalloc_rejects_meshes_above_the_scratch_size():
@@ -111,3 +156,21 @@ def test_noalloc_rejects_meshes_above_the_scratch_size():
                                    None, None, None)
     assert rc == N.EINVAL
     assert b"65536" in N.lib().hcfd_last_error()
+
+
+@pytest.mark.parametrize("kw", [dict(bc_first=[140, 155, 160]), dict(bc_first=[150, 155, 159]),
+                                dict(bc_first=[150, 161, 160]), dict(nbc=0, bc_first=[0]),
+                                dict(F_BC=160, nbc=1, bc_first=[150, 160])])
+def test_noalloc_rejects_a_boundary_table_that_does_not_cover_the_boundary_faces(kw):
+    """Checked on the host before any CUDA call: runs without a GPU."""
+    m, keep = _bad_mesh(**kw)
+    assert _call(m) == N.EINVAL
+    assert b"bc_first" in N.lib().hcfd_last_error() or b"boundary colours" in N.lib().hcfd_last_error()
+
+
+@pytest.mark.parametrize("U_in,U_out", [(4096, 4096), (4096, 4096 + 8), (4096 + 3200 - 8, 4096)])
+def test_noalloc_rejects_overlapping_state_buffers(U_in, U_out):
+    """4 Nc doubles (3,200 bytes at Nc = 100) from each pointer: any shared byte is refused."""
+    m, keep = _bad_mesh()
+    assert _call(m, U_in, U_out) == N.EINVAL
+    assert b"overlap" in N.lib().hcfd_last_error()
