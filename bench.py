@@ -312,7 +312,13 @@ def main():
                     help="step kernel family (the per-cell gather kernels are the other fusion split)")
     ap.add_argument("--profile-only", action="store_true",
                     help="warm-up and timed steps only (no end-to-end, variants, CPU, batched or served legs): for ncu")
+    ap.add_argument("--tour", action="store_true",
+                    help="run every kernel of the library a few times (default mesh 1025x513) for a launch list")
     args = ap.parse_args()
+    if args.tour:
+        nx, ny = (int(x) for x in (args.mesh if args.mesh != f"{NX}x{NY}" else "1025x513").lower().split("x"))
+        print(json.dumps(run_tour(nx, ny)), flush=True)
+        return 0
     NX, NY = (int(x) for x in args.mesh.lower().split("x"))
     if args.profile_only:
         args.no_cpu = args.no_variants = args.no_batched = args.no_served = True
@@ -436,6 +442,82 @@ def main():
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+# ---------------------------------------------------------------------------------------
+# --tour: every kernel of the library a few times on one mid-sized case, so that one
+# profiler run (a launch list of device times) covers all of them.  Single mesh: a
+# 1025 x 513-node wedge (1,048,576 triangles, RCM numbering, Venkatakrishnan K = 5, M 2.5),
+# the tiled FP64 and FP32 solvers and the per-cell FP64 and FP32 solvers, each through set-up
+# (geometry, renumbering, face records), initialise and boundary cells, steps in global and
+# local CFL mode, an asynchronous snapshot, download, upload, the wall pressure coefficient
+# and a checkpoint / restore.  Arena: `instances` wedges of 10,000 to 60,000 triangles
+# admitted to one FP32 arena (admission kernels), stepped, polled, fetched, checkpointed,
+# restored and released.  Prints one JSON line with the cells touched and the steps taken.
+
+def _tour_single(H, mesh, precision: int, kernel: int, steps: int, tmp: str) -> dict:
+    bcmap, qbc, q = H.wedge_case(2.5)
+    s = H.Solver(mesh, limiter=H.LIMITER_VENKAT, venkat_K=5.0, precision=precision, kernel=kernel)
+    s.gather_bcs(bcmap, qbc)
+    s.initialise(q)
+    s.step(steps, H.GLOBAL_CFL, 0.5)
+    s.step(steps, H.LOCAL_CFL, 0.5)
+    out = np.empty((4, mesh.Nc), dtype=np.float64)
+    s.snapshot(out, prims=True).wait()
+    U = s.U()
+    s.upload(U)
+    s.wall_cp(2, q[0], q[3], float(np.hypot(q[1], q[2])))    # colour 2: the ramp
+    path = os.path.join(tmp, "tour.ckpt")
+    s.checkpoint(path)
+    s.restore(path)
+    s.step(1, H.GLOBAL_CFL, 0.5)
+    H.device_sync()
+    st = s.stats()
+    del s
+    return dict(cells=mesh.Nc, faces=mesh.Nf, steps=2 * steps + 1, residual_l2=st["res_l2"])
+
+
+def _tour_arena(H, n: int, steps: int, tmp: str, seed: int = 7) -> dict:
+    from cfd_optimisations_b200.arena import Arena
+    rng = np.random.default_rng(seed)
+    a = Arena(int(2e9), precision=H.FP32, limiter=H.LIMITER_BJ, max_instances=n + 8)
+    slots, cells = [], 0
+    for i in range(n):
+        ntri = float(np.exp(rng.uniform(np.log(1e4), np.log(6e4))))
+        ny1 = max(2, int(round(np.sqrt(ntri / 4.0))))
+        m = H.Mesh.wedge(2 * ny1 + 1, ny1 + 1, theta_deg=float(rng.uniform(5.0, 15.0)), seed=100 + i,
+                         numbering=H.NUMBER_RANDOM)
+        bcmap, qbc, q = H.wedge_case(float(rng.uniform(1.8, 4.0)))
+        k = a.admit(m, bcmap, qbc, q, 0.5)
+        if k is None:
+            raise RuntimeError("arena full")
+        slots.append(k)
+        cells += m.Nc
+    a.step(steps)
+    a.poll()
+    a.fetch(slots[0])
+    path = os.path.join(tmp, "tour_arena.ckpt")
+    a.checkpoint(slots[0], path)
+    a.restore(slots[0], path)
+    a.step(2)
+    a.poll()
+    for k in slots:
+        a.release(k)
+    H.device_sync()
+    del a
+    return dict(instances=n, cells=cells, steps=steps + 2)
+
+
+def run_tour(nx: int = 1025, ny: int = 513, steps: int = 3, instances: int = 64) -> dict:
+    import cfd_optimisations_b200 as H
+    mesh = H.Mesh.wedge(nx, ny, theta_deg=15.0, seed=1234, numbering=H.NUMBER_RCM)
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, prec, kern in (("tiled_fp64", H.FP64, H.KERNEL_TILED), ("tiled_fp32", H.FP32, H.KERNEL_TILED),
+                                 ("cell_fp64", H.FP64, H.KERNEL_CELL), ("cell_fp32", H.FP32, H.KERNEL_CELL)):
+            out[name] = _tour_single(H, mesh, prec, kern, steps, tmp)
+        out["arena_fp32"] = _tour_arena(H, instances, steps, tmp)
+    return out
 
 
 if __name__ == "__main__":

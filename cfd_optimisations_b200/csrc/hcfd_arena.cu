@@ -309,6 +309,8 @@ hcfd::TileArgs<T> arena_args(hcfd_arena* A, int cur, int par) {
     a.Hmax = A->Hcur;
     a.Fmax = A->Fcur;
     a.err = A->err;
+    a.polls = 1u << 22;
+    a.skip_tile = -1;
     a.ps = (int) A->Ccap;
     a.tiles = A->tiles;
     a.inst_dt = A->inst_dt;

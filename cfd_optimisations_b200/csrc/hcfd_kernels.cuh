@@ -171,11 +171,11 @@ __device__ __forceinline__ float qsqrt<float>(float x) { return x == 0.0f ? 0.0f
 // ---------------------------------------------------------------------------------------
 // flux arithmetic, written with the reference's expression trees
 
-// Flux::EulerFlux (src/Base/Flux.cpp:89-97).
+// Flux::EulerFlux (src/Base/Flux.cpp:89-97); ir = 1/U[0], which Rusanov has formed already
+// (the same IEEE quotient, so passing it on changes no bit).
 template <class T>
-__device__ __forceinline__ void euler_flux(const T U[4], T n0, T n1, T gma, T F[4]) {
+__device__ __forceinline__ void euler_flux(const T U[4], T ir, T n0, T n1, T gma, T F[4]) {
     const T gmo = gma - T(1);
-    const T ir = qrcp(U[0]);
     const T P = gmo * (U[3] - T(0.5) * ir * (U[1] * U[1] + U[2] * U[2]));
     F[0] = n0 * U[1] + n1 * U[2];
     F[1] = n0 * (U[1] * U[1] * ir + P) + n1 * U[2] * U[1] * ir;
@@ -201,8 +201,8 @@ __device__ __forceinline__ void rusanov(const T UL[4], const T UR[4], T n0, T n1
     const T S2 = fmax(fabs(nvl + al), fabs(nvr + ar));
     const T S = fmax(S1, S2);
     T FL[4], FR[4];
-    euler_flux(UL, n0, n1, gma, FL);
-    euler_flux(UR, n0, n1, gma, FR);
+    euler_flux(UL, irl, n0, n1, gma, FL);
+    euler_flux(UR, irr, n0, n1, gma, FR);
 #pragma unroll
     for (int v = 0; v < 4; v++) F[v] = T(0.5) * ((FL[v] + FR[v]) - S * (UR[v] - UL[v]));
 }
@@ -223,13 +223,34 @@ __device__ __forceinline__ void cell_speed(const T U[4], T gma, T& u, T& v, T& a
     a = qsqrt(gma * p * ir);
 }
 
-// Venkatakrishnan face limiter for one side: min(1, (D1^2 + e2 + 2 D1 d)/(D1^2 + 2 d^2 +
-// D1 d + e2)), e2 = (K h)^3, h = sqrt(cell area).
+// Face value of the limiter for one variable, |d| > 1e-9 (d = grad u . r_f):
+//   Barth-Jespersen (Limiter.cpp:67-71): min(1, D1 / d), D1 = u_max - u if d > 0, else u_min - u;
+//   Venkatakrishnan: min(1, (D1^2 + e2 + 2 D1 d) / (D1^2 + 2 d^2 + D1 d + e2)),
+//                    e2 = (K h)^3, h = sqrt(cell area).
+// The quotient is formed only where it can be below 1.  Where the exact quotient is at least 1
+// (BJ: D1 and d share their sign and |D1| >= |d|; Venkatakrishnan: num >= den, den > 0) its
+// rounding is at least 1 too, and min(1, .) gives 1: skipping the division there gives the
+// same bits as always dividing.  (FP32's approximate division could give one ulp below 1
+// where num = den; the skip gives 1 there, the IEEE value.)
+// In FP32 the approximate quotient costs two instructions, less than a branch around it: it
+// is always formed and the result selected.
 template <class T>
-__device__ __forceinline__ T venkat(T D1, T d, T e2) {
-    const T num = D1 * D1 + e2 + T(2) * D1 * d;
-    const T den = D1 * D1 + T(2) * d * d + D1 * d + e2;
-    return fmin(T(1), qdiv(num, den));
+__device__ __forceinline__ T face_limiter(int limiter, T D1, T d, T e2) {
+    T num = D1, den = d;
+    bool ge1;
+    if (limiter == LIM_BJ) {
+        ge1 = d > T(0) ? D1 >= d : D1 <= d;
+    } else {
+        num = D1 * D1 + e2 + T(2) * D1 * d;
+        den = D1 * D1 + T(2) * d * d + D1 * d + e2;
+        ge1 = num >= den;
+    }
+    if constexpr (sizeof(T) == 4) {
+        const T q = fmin(T(1), qdiv(num, den));
+        return ge1 ? T(1) : q;
+    } else {
+        return ge1 ? T(1) : fmin(T(1), qdiv(num, den));
+    }
 }
 
 // Two-sum accumulation s + c += x (Knuth), with explicit round-to-nearest adds so that no
@@ -366,13 +387,9 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
                     for (int k = 0; k < W; k++) {
                         if (s[k].y < 0) continue;
                         const T d = gx * ro[k][0] + gy * ro[k][1];   // Limiter.cpp:50-51
-                        T pf = T(1);
-                        if (a.limiter == LIM_BJ) {                   // Limiter.cpp:67-71
-                            // one division: the numerator is picked by the sign of d
-                            if (d > eps || d < -eps) pf = fmin(T(1), qdiv((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d));
-                        } else {
-                            if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
-                        }
+                        T pf = T(1);                                 // Limiter.cpp:67-71
+                        if (d > eps || d < -eps)
+                            pf = face_limiter(a.limiter, (d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
                         phi = fmin(phi, pf);                         // Limiter.cpp:73-74
                     }
                 }

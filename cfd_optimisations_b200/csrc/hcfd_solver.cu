@@ -119,6 +119,10 @@ struct hcfd_solver {
     double ms1 = 0, ms2 = 0;
     long long n1 = 0, n2 = 0;
 
+    // bounded waits of the tiled kernels (hcfd_gpu_test_waits changes them for tests)
+    unsigned wait_polls = 1u << 22;
+    int wait_skip_tile = -1;
+
     bool fp32() const { return prm.precision == HCFD_FP32; }
 };
 
@@ -188,6 +192,8 @@ hcfd::TileArgs<T> tile_args(hcfd_solver* s, int time_mode, double dt_or_cfl, con
     a.Hmax = P.plan.Hmax;
     a.Fmax = P.plan.Fmax;
     a.err = s->d_err;
+    a.polls = s->wait_polls;
+    a.skip_tile = s->wait_skip_tile;
     a.ps = s->Nc;
     a.tiles = nullptr;
     a.inst_dt = nullptr;
@@ -663,6 +669,21 @@ int hcfd_gpu_step(hcfd_solver* s, int nsteps, int time_mode, double dt_or_cfl, h
         }
     }
     if (stats) return read_stats(s, stats);
+    return HCFD_OK;
+}
+
+int hcfd_gpu_test_waits(hcfd_solver* s, unsigned polls, int skip_tile) {
+    hcfd::clear_error();
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (polls > (1u << 30)) return fail(HCFD_EINVAL, "test_waits: poll limit above 2^30");
+    s->wait_polls = polls ? polls : (1u << 22);
+    s->wait_skip_tile = skip_tile < 0 ? -1 : skip_tile;
+    if (s->graph) {                      // the kernel arguments live in the graph
+        CK(cudaStreamSynchronize(s->stream));
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
     return HCFD_OK;
 }
 

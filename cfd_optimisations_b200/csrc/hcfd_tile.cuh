@@ -26,7 +26,10 @@ struct TileArgs {
     const int* __restrict__ halo;          // internal cell ids
     const short* __restrict__ cslot;       // [ntiles * B * Wp]: (entry << 1) | cell-is-right, or -1; Wp = W
     int ntiles, B, Wp, Hmax, Fmax;
-    unsigned int* err;                     // bit 0: a bounded wait gave up
+    unsigned int* err;                     // bit 0: a bounded wait gave up; bit 1: copies did not drain
+    unsigned polls;                        // poll limit of every bounded wait (2^22 by default)
+    int skip_tile;                         // failure injection for tests: the producer arms nothing
+                                           // for this tile (-1: none)
     int ps;                                // plane stride of the cell planes (Nc, or the arena's capacity)
     // Arena mode (many meshes in one flat arena; see hcfd_arena.cu).  Tile i of the active
     // list is described by tiles[2i] = {first cell, first entry, entries, instance} and
@@ -68,7 +71,10 @@ struct StageInfo {
     long long pad2;
 };
 static_assert(sizeof(StageInfo) == 64, "stage info is 64 bytes");
-constexpr int kHeader = 256;   // full[4], empty[4] mbarriers, then StageInfo per stage (two)
+// Header of a CTA's shared memory: full[2] and empty[2] mbarriers (bytes 0-31), the abort
+// words (32-39), then StageInfo per stage (two, from byte 64).
+constexpr int kHeader = 256;
+constexpr unsigned kDrainPolls = 1u << 24;
 
 // ---------------------------------------------------------------------------------------
 // PTX helpers (sm_90+ bulk copies and mbarriers; sm_80+ cp.async)
@@ -97,21 +103,42 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
                  : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
     return ok != 0;
 }
-// Bounded wait for an mbarrier phase: gives up after ~2^22 polls, records the failure and
-// returns false (the kernel then finishes its tile loop with whatever data it has; the
-// host reports HCFD_ETIMEOUT).
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned int* err) {
+// Bounded wait for an mbarrier phase.  Gives up after `polls` polls, or early once another
+// thread of the CTA has given up (its abort word is set); on giving up it records the failure
+// in the kernel's error word (the host reports HCFD_ETIMEOUT) and in the abort word, and
+// returns false.  A thread whose wait failed never reads the stage it waited for: the
+// producer then stops issuing copies, and the consumers leave their tile loop (see
+// producer_loop and HCFD_TILE_LOOP_BEGIN).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned polls, unsigned int* err,
+                                          volatile int* abort) {
 #pragma unroll 1
-    for (int i = 0; i < (1 << 22); i++)
+    for (unsigned i = 0; i < polls; i++) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 255u) == 255u && *abort) return false;
+    }
     atomicOr(err, 1u);
+    *abort = 1;
     return false;
+}
+// Bounded wait for copies already issued (they only read valid global memory, so they land);
+// used before a CTA exits so that nothing is written into its shared memory afterwards.
+__device__ __forceinline__ void mbar_drain(unsigned long long* bar, unsigned parity, unsigned int* err) {
+#pragma unroll 1
+    for (unsigned i = 0; i < kDrainPolls; i++)
+        if (mbar_try_wait(bar, parity)) return;
+    atomicOr(err, 2u);
 }
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ volatile int* abort_word(unsigned char* smem) { return reinterpret_cast<volatile int*>(smem + 32); }
+// Set by compute threads only, before the compute barrier that follows the stage wait
+// (pass 2): read after that barrier, every compute warp sees the same value.
+__device__ __forceinline__ volatile int* compute_abort_word(unsigned char* smem) {
+    return reinterpret_cast<volatile int*>(smem + 36);
 }
 
 // Shared-memory loads (plain loads: the __ldg helpers of hcfd_kernels.cuh are global-only).
@@ -141,6 +168,12 @@ template <class T>
 __device__ __forceinline__ void lds_geo(const T* p, int nf, int e, FaceGeo<T>& g) {
     g.nx = p[e]; g.ny = p[nf + e]; g.Af = p[2 * nf + e]; g.If = p[3 * nf + e];
     g.rLx = p[4 * nf + e]; g.rLy = p[5 * nf + e]; g.rRx = p[6 * nf + e]; g.rRy = p[7 * nf + e];
+}
+
+// Normal, length and interpolation weight (pass 1 reads the r vector of one side apart).
+template <class T>
+__device__ __forceinline__ void lds_geo4(const T* p, int nf, int e, FaceGeo<T>& g) {
+    g.nx = p[e]; g.ny = p[nf + e]; g.Af = p[2 * nf + e]; g.If = p[3 * nf + e];
 }
 
 // Normal and length only (the components pass 2's flux write leaves intact).
@@ -192,15 +225,21 @@ __device__ __forceinline__ void compute_sync(int nthreads) {
 // cp.async and signals their completion on the same mbarrier.  The `full` barrier therefore
 // completes when all of the tile's data has landed: 1 expect-tx arrival + 32 cp.async
 // arrivals + the transaction bytes.
+// Once any wait of the CTA has given up, the producer issues nothing more; before it
+// returns it waits for the copies it has issued (the last armed phase of each buffer; earlier
+// ones completed before their buffer was re-armed), so no copy lands after the CTA exits.
 template <class T, bool PASS2, bool ARENA>
 __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned char* smem, unsigned long long* full,
                                               unsigned long long* empty, const TileSmem<T>& L) {
     const int lane = threadIdx.x & 31;
     constexpr int CU = sizeof(Cell4<T>) / 16, CG = PASS2 ? sizeof(Grad8<T>) / 16 : 0;
     const int NL = a.B + a.Hmax;   // plane stride of the staged cells
+    volatile int* abort = abort_word(smem);
+    int armed[2] = {-1, -1};       // last iteration whose copies were issued into each buffer
     unsigned iter = 0;
     for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {
         const int buf = iter & 1;
+        if (__any_sync(0xffffffffu, *abort)) break;
         // the tile's descriptor and its instance's scalars are loaded before the wait for the
         // stage, so that their latency hides behind it (none of them changes during the kernel
         // in a way the kernel reads: dt minima and step counts come from earlier kernels)
@@ -222,7 +261,9 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
                 v_steps = a.s.stats->steps;
             }
         }
-        if (iter >= 2) mbar_wait(empty + buf, ((iter >> 1) - 1) & 1, a.err);
+        if (iter >= 2 && !__all_sync(0xffffffffu, mbar_wait(empty + buf, ((iter >> 1) - 1) & 1, a.polls, a.err, abort)))
+            break;
+        if (t == a.skip_tile) continue;      // failure injection: nothing armed, nothing in flight
         unsigned char* st = smem + kHeader + buf * L.stage;
         Cell4<T>* sU = reinterpret_cast<Cell4<T>*>(st + L.u);
         Grad8<T>* sG = reinterpret_cast<Grad8<T>*>(st + L.g);
@@ -270,7 +311,11 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
                            reinterpret_cast<const char*>(a.s.phiG) + 16 * ((size_t) j * a.ps + ci));
         }
         cp_async_arrive_noinc(full + buf);
+        armed[buf] = (int) iter;
     }
+    cp_async_wait_all();
+    for (int b = 0; b < 2; b++)
+        if (armed[b] >= 0) mbar_drain(full + b, ((unsigned) armed[b] >> 1) & 1, a.err);
 }
 
 // Residual / non-finite / dt bookkeeping shared by the last pass of a step.
@@ -390,6 +435,11 @@ struct FaceIn {
 // (producer_loop); the first NT = blockDim.x - 32 threads compute.  Compute iteration i
 // reads staging buffer i & 1 once its `full` barrier completes and releases it on its
 // `empty` barrier (one arrival per compute warp) when done.
+// A compute warp whose stage wait gives up reads nothing of that stage.  In pass 1 (no
+// barrier among the compute warps inside the loop) it leaves the loop at once.  In pass 2
+// it marks the compute abort word and skips the face phase (`staged` false); every compute
+// warp then meets at the compute barrier that ends the face phase and leaves the loop
+// there if any of them gave up, so none is left waiting at that barrier.
 #define HCFD_TILE_LOOP_BEGIN(PASS2, ARENA)                                                       \
     const int NT = blockDim.x - 32;                                                              \
     const int NL = a.B + a.Hmax;                                                                 \
@@ -398,6 +448,8 @@ struct FaceIn {
     if (threadIdx.x == 0) {                                                                      \
         mbar_init(full, 33); mbar_init(full + 1, 33);                                            \
         mbar_init(empty, NT / 32); mbar_init(empty + 1, NT / 32);                                \
+        *abort_word(smem) = 0;                                                                   \
+        *compute_abort_word(smem) = 0;                                                           \
         fence_mbar_init();                                                                       \
     }                                                                                            \
     __syncthreads();                                                                             \
@@ -408,7 +460,11 @@ struct FaceIn {
     for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {                             \
         const int buf = iter & 1;                                                                \
         unsigned char* st = smem + kHeader + buf * L.stage;                                      \
-        mbar_wait(full + buf, (iter >> 1) & 1, a.err);                                           \
+        const bool staged = __all_sync(0xffffffffu,                                              \
+                                       mbar_wait(full + buf, (iter >> 1) & 1, a.polls, a.err,    \
+                                                 abort_word(smem)));                             \
+        if (!PASS2 && !staged) break;                                                            \
+        if (PASS2 && !staged && (threadIdx.x & 31) == 0) *compute_abort_word(smem) = 1;          \
         const StageInfo& si = reinterpret_cast<const StageInfo*>(smem + 64)[buf];                \
         const int base = si.base, nb = si.nb, h0t = si.h0, inst = si.inst;                      \
         const Cell4<T>* sU = reinterpret_cast<const Cell4<T>*>(st + L.u);                        \
@@ -451,8 +507,8 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
             const int e = cs[k] >> 1;
             const bool isL = (cs[k] & 1) == 0;
             FaceGeo<T> g;
-            lds_geo(sGeo, nfl, e, g);
-            const int nbl = isL ? sMeta[4 * e + 1] : sMeta[4 * e];
+            lds_geo4(sGeo, nfl, e, g);
+            const int nbl = sMeta[4 * e + (isL ? 1 : 0)];
             T un[4];
             lds_cell(sU, NL, nbl, un);
 #pragma unroll
@@ -467,8 +523,9 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
                 umin[v] = fmin(umin[v], un[v]);
                 umax[v] = fmax(umax[v], un[v]);
             }
-            ro[k][0] = isL ? g.rLx : g.rRx;
-            ro[k][1] = isL ? g.rLy : g.rRy;
+            // this cell's own centre-to-face vector: one pair of loads at the side's offset
+            ro[k][0] = sGeo[(isL ? 4 : 6) * nfl + e];
+            ro[k][1] = sGeo[(isL ? 5 : 7) * nfl + e];
             if (s.time_mode != TM_FIXED) lam += wave(cu, cv, ca, g);
         }
         T e2 = T(0);
@@ -490,13 +547,9 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
                 for (int k = 0; k < W; k++) {
                     if (cs[k] < 0) continue;
                     const T d = gx * ro[k][0] + gy * ro[k][1];
-                    T pf = T(1);
-                    if (s.limiter == LIM_BJ) {                       // Limiter.cpp:67-71
-                        // one division: the numerator is picked by the sign of d
-                        if (d > eps || d < -eps) pf = fmin(T(1), qdiv((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d));
-                    } else {
-                        if (d > eps || d < -eps) pf = venkat((d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
-                    }
+                    T pf = T(1);                                     // Limiter.cpp:67-71
+                    if (d > eps || d < -eps)
+                        pf = face_limiter(s.limiter, (d > eps) ? umax[v] - u[v] : umin[v] - u[v], d, e2);
                     phi = fmin(phi, pf);
                 }
             }
@@ -549,7 +602,7 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
     const T cfl_or_dt = T(si.dt_or_cfl);
     dt_used = (s.time_mode == TM_FIXED) ? si.dt_or_cfl : si.dt_or_cfl * si.dtmin;
     const Grad8<T>* sG = reinterpret_cast<const Grad8<T>*>(st + L.g);
-    const int nf = nfl;
+    const int nf = staged ? nfl : 0;         // a stage whose wait gave up is not read
     // face phase: one Rusanov flux per face entry (Flux.cpp:19-38).  Each thread takes two
     // entries per round and computes both before storing either, so the two independent
     // FP64 dependency chains (divisions, square roots) interleave.
@@ -582,6 +635,7 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
         }
     }
     compute_sync(NT);
+    if (*compute_abort_word(smem)) break;    // some compute warp's stage wait gave up
     // cell phase: slots in increasing face order, update, ghost refresh
     for (int c = threadIdx.x; c < nb; c += NT) {
         short cs[8];

@@ -96,6 +96,7 @@ _SIGS = {
     "hcfd_gpu_upload": (ct.c_int, [ct.c_void_p, ct.POINTER(_dp)]),
     "hcfd_gpu_sync": (ct.c_int, [ct.c_void_p]),
     "hcfd_gpu_stats": (ct.c_int, [ct.c_void_p, ct.POINTER(StepStats)]),
+    "hcfd_gpu_test_waits": (ct.c_int, [ct.c_void_p, ct.c_uint, ct.c_int]),
     "hcfd_gpu_wall_cp": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double, ct.c_double, ct.c_double, _dp, _ip]),
     "hcfd_gpu_info": (ct.c_int, [ct.c_void_p, _ip, _ip, _ip, _ip]),
     "hcfd_gpu_profile": (ct.c_int, [ct.c_void_p, ct.c_int]),

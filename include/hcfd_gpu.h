@@ -219,6 +219,14 @@ int  hcfd_gpu_sync(hcfd_solver* s);
 /* Statistics of the steps taken so far (waits for the stream; no reference counterpart:
  * the reference computes no residual). */
 int  hcfd_gpu_stats(hcfd_solver* s, hcfd_step_stats* stats);
+/* Failure injection for tests of the bounded waits (no reference counterpart: the reference
+ * has no device and no waits).  Every wait of the tiled step kernels gives up after `polls`
+ * polls (0 restores the default, 2^22; at most 2^30); with skip_tile >= 0 the staging warp
+ * arms and copies nothing for that tile, so the wait for it runs out with no copy in flight.
+ * The next step then returns HCFD_ETIMEOUT with the state partly stepped; the kernels leave
+ * no copy in flight and the context stays usable: hcfd_gpu_initialise clears the error, and
+ * with the hook reset (polls 0, skip_tile -1) the handle steps normally again. */
+int  hcfd_gpu_test_waits(hcfd_solver* s, unsigned polls, int skip_tile);
 /* Wall pressure coefficient (p_CL - p_inf) / (0.5 rho_inf |u_inf|^2) on the faces of one
  * colour, in face order; *n gets the face count.  No reference counterpart. */
 int  hcfd_gpu_wall_cp(hcfd_solver* s, int colour, double rho_inf, double p_inf, double speed_inf,

@@ -30,8 +30,19 @@ ORACLE32_SO = os.path.join(HERE, "_build", "libhcfd_oracle32.so")
 ORACLE32NC_SO = os.path.join(HERE, "_build", "libhcfd_oracle32nc.so")
 MESH_SO = os.path.join(HERE, "_build", "libhcfd_oracle_mesh.so")
 REF_SO = os.path.join(HERE, "_ref", "libhcfd_ref.so")
-# where the reference sources lie when they are present (the Makefile's REF default)
-REF_DIR = os.environ.get("HCFD_REFERENCE", "/root/reference")
+
+
+def _reference_dir() -> str:
+    """Where the reference sources lie: $HCFD_REFERENCE, else a checkout named `reference`
+    beside this repository; "" when neither holds the reference's sources."""
+    for d in (os.environ.get("HCFD_REFERENCE", ""),
+              os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")):
+        if d and os.path.exists(os.path.join(d, "src", "Mesh.cpp")):
+            return d
+    return ""
+
+
+REF_DIR = _reference_dir()
 
 # includes/Base/BoundaryConditions.hpp:6-13
 SYMMETRY, WALL, SUPINLET, SUBINLET, SUPOUTLET, SUBOUTLET = range(6)
@@ -53,8 +64,8 @@ def _i(a):
 
 
 def build(ref: bool = True) -> None:
-    """Builds the oracle (and, when the reference sources exist, the reference library)."""
-    targets = ["oracle"] + (["ref"] if ref and os.path.isdir(os.path.join(REF_DIR, "src")) else [])
+    """Builds the oracle (and, when the reference sources are found, the reference library)."""
+    targets = ["oracle"] + ([f"REF={REF_DIR}", "ref"] if ref and REF_DIR else [])
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 

@@ -1,7 +1,7 @@
-"""Regenerates the committed fixtures of this directory (run in a container that has the
-reference sources at /root/reference and oracle/_ref built):
+"""Regenerates the committed fixtures of this directory (run where the reference's sources and
+oracle/_ref, the reference built from them, are present):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference source tree>
 
 * wedge.hmsh, Base_0.hsln, Base_1.hsln — the reference's own mesh and its shipped golden
   solutions (sols/Base_{0,1}.hsln: the initial state and the state after exactly 1000
@@ -20,12 +20,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 
-def main():
+def main(REF: str):
     import oracle as O
     import cfd_optimisations_b200 as H
 
@@ -59,4 +58,6 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2 or not os.path.exists(os.path.join(sys.argv[1], "sols")):
+        sys.exit("usage: make_golden.py <reference source tree>")
+    main(sys.argv[1])
