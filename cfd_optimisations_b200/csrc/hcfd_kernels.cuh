@@ -227,30 +227,14 @@ __device__ __forceinline__ void cell_speed(const T U[4], T gma, T& u, T& v, T& a
 //   Barth-Jespersen (Limiter.cpp:67-71): min(1, D1 / d), D1 = u_max - u if d > 0, else u_min - u;
 //   Venkatakrishnan: min(1, (D1^2 + e2 + 2 D1 d) / (D1^2 + 2 d^2 + D1 d + e2)),
 //                    e2 = (K h)^3, h = sqrt(cell area).
-// The quotient is formed only where it can be below 1.  Where the exact quotient is at least 1
-// (BJ: D1 and d share their sign and |D1| >= |d|; Venkatakrishnan: num >= den, den > 0) its
-// rounding is at least 1 too, and min(1, .) gives 1: skipping the division there gives the
-// same bits as always dividing.  (FP32's approximate division could give one ulp below 1
-// where num = den; the skip gives 1 there, the IEEE value.)
-// In FP32 the approximate quotient costs two instructions, less than a branch around it: it
-// is always formed and the result selected.
+// (Skipping the quotient where it is at least 1 would give the same bits, but measured on the
+// B200 the branch costs more than the division it saves, in both precisions.)
 template <class T>
 __device__ __forceinline__ T face_limiter(int limiter, T D1, T d, T e2) {
-    T num = D1, den = d;
-    bool ge1;
-    if (limiter == LIM_BJ) {
-        ge1 = d > T(0) ? D1 >= d : D1 <= d;
-    } else {
-        num = D1 * D1 + e2 + T(2) * D1 * d;
-        den = D1 * D1 + T(2) * d * d + D1 * d + e2;
-        ge1 = num >= den;
-    }
-    if constexpr (sizeof(T) == 4) {
-        const T q = fmin(T(1), qdiv(num, den));
-        return ge1 ? T(1) : q;
-    } else {
-        return ge1 ? T(1) : fmin(T(1), qdiv(num, den));
-    }
+    if (limiter == LIM_BJ) return fmin(T(1), qdiv(D1, d));
+    const T num = D1 * D1 + e2 + T(2) * D1 * d;
+    const T den = D1 * D1 + T(2) * d * d + D1 * d + e2;
+    return fmin(T(1), qdiv(num, den));
 }
 
 // Two-sum accumulation s + c += x (Knuth), with explicit round-to-nearest adds so that no

@@ -19,7 +19,7 @@ namespace hcfd {
 template <class T>
 struct TileArgs {
     StepArgs<T> s;                         // state, stats, BC table, modes
-    const T* __restrict__ tgeo;            // face records, per tile component-major: [8][nf]
+    const T* __restrict__ tgeo;            // face records, per tile pair-major: [4][nf] pairs
     const short* __restrict__ tmeta;       // 4 shorts per entry: la, lb, bc, 0
     const int* __restrict__ foff;          // [ntiles + 1], multiples of 4
     const int* __restrict__ hoff;          // [ntiles + 1]
@@ -162,24 +162,45 @@ __device__ __forceinline__ void lds_grad(const Grad8<float>* p, int ps, int i, f
     const float4 a = q[i], b = q[ps + i];
     g[0] = a.x; g[1] = a.y; g[2] = a.z; g[3] = a.w; g[4] = b.x; g[5] = b.y; g[6] = b.z; g[7] = b.w;
 }
-// Face record e of a tile whose records are stored component-major ([8][nf]): consecutive
-// threads reading consecutive records touch consecutive words (no bank conflicts).
+// Face records of a tile are stored pair-major: four planes of pairs, (nx, ny), (Af, If),
+// (rLx, rLy), (rRx, rRy); pair j of entry e at index j nf + e of the pair array (16 bytes a pair
+// in double, 8 in float).  One load brings a pair, and consecutive threads reading consecutive
+// entries touch consecutive words (no bank conflicts).
+template <class T> struct PairOf;
+template <> struct PairOf<double> { using type = double2; };
+template <> struct PairOf<float> { using type = float2; };
+template <class T>
+__device__ __forceinline__ typename PairOf<T>::type ldp(const T* p, int nf, int j, int e) {
+    return reinterpret_cast<const typename PairOf<T>::type*>(p)[j * nf + e];
+}
+template <class T>
+__device__ __forceinline__ void stp(T* p, int nf, int j, int e, T x, T y) {
+    typename PairOf<T>::type v;
+    v.x = x; v.y = y;
+    reinterpret_cast<typename PairOf<T>::type*>(p)[j * nf + e] = v;
+}
+// The length A_f alone (first half of pair 1).
+template <class T>
+__device__ __forceinline__ T lds_area(const T* p, int nf, int e) { return p[2 * (nf + e)]; }
+
 template <class T>
 __device__ __forceinline__ void lds_geo(const T* p, int nf, int e, FaceGeo<T>& g) {
-    g.nx = p[e]; g.ny = p[nf + e]; g.Af = p[2 * nf + e]; g.If = p[3 * nf + e];
-    g.rLx = p[4 * nf + e]; g.rLy = p[5 * nf + e]; g.rRx = p[6 * nf + e]; g.rRy = p[7 * nf + e];
+    const auto a = ldp(p, nf, 0, e), b = ldp(p, nf, 1, e), c = ldp(p, nf, 2, e), d = ldp(p, nf, 3, e);
+    g.nx = a.x; g.ny = a.y; g.Af = b.x; g.If = b.y; g.rLx = c.x; g.rLy = c.y; g.rRx = d.x; g.rRy = d.y;
 }
 
 // Normal, length and interpolation weight (pass 1 reads the r vector of one side apart).
 template <class T>
 __device__ __forceinline__ void lds_geo4(const T* p, int nf, int e, FaceGeo<T>& g) {
-    g.nx = p[e]; g.ny = p[nf + e]; g.Af = p[2 * nf + e]; g.If = p[3 * nf + e];
+    const auto a = ldp(p, nf, 0, e), b = ldp(p, nf, 1, e);
+    g.nx = a.x; g.ny = a.y; g.Af = b.x; g.If = b.y;
 }
 
 // Normal and length only (the components pass 2's flux write leaves intact).
 template <class T>
 __device__ __forceinline__ void lds_geo3(const T* p, int nf, int e, T& nx, T& ny, T& Af) {
-    nx = p[e]; ny = p[nf + e]; Af = p[2 * nf + e];
+    const auto a = ldp(p, nf, 0, e);
+    nx = a.x; ny = a.y; Af = lds_area(p, nf, e);
 }
 
 __host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~size_t(127); }
@@ -389,7 +410,7 @@ __device__ __forceinline__ void lds_slots(const short* p, int Wp, short cs[8]) {
 // L -> R orientation.  Only the reconstructed states stay live between load and flux.
 template <class T>
 struct FaceIn {
-    T uoL[4], uqR[4], nx, ny;
+    T uoL[4], uqR[4], nx, ny, Af;
     int e;
     __device__ __forceinline__ void load(const Cell4<T>* sU, const Grad8<T>* sG, int NL, const T* sGeo,
                                          const short* sMeta, int nf, int e_) {
@@ -398,7 +419,7 @@ struct FaceIn {
         const int bc = m.z;
         FaceGeo<T> g;
         lds_geo(sGeo, nf, e, g);
-        nx = g.nx; ny = g.ny;
+        nx = g.nx; ny = g.ny; Af = g.Af;
         T uL[4], uR[4], gL[8];
         lds_cell(sU, NL, m.x, uL);
         lds_cell(sU, NL, m.y, uR);
@@ -423,11 +444,19 @@ struct FaceIn {
         }
     }
     __device__ __forceinline__ void flux(T gma, T F[4]) const { rusanov(uoL, uqR, nx, ny, gma, F); }
-    // F over components 3..6 (If, rLx, rLy, rRx) of this entry's staged record: only this
-    // thread reads them in pass 2, and it has read them already.
+    // F over pairs 2 and 3 (the r vectors) of this entry's staged record: only this thread
+    // reads them in pass 2, and it has read them already.  With AF the product A_f F is stored
+    // instead (the compensated FP32 sums round that product before adding it, so forming it
+    // once per face gives the same bits as forming it in each of the two cells).
+    template <bool AF>
     __device__ __forceinline__ void store(T* sGeo, int nf, const T F[4]) const {
-#pragma unroll
-        for (int v = 0; v < 4; v++) sGeo[(3 + v) * nf + e] = F[v];
+        if (AF) {
+            stp(sGeo, nf, 2, e, F[0] * Af, F[1] * Af);
+            stp(sGeo, nf, 3, e, F[2] * Af, F[3] * Af);
+        } else {
+            stp(sGeo, nf, 2, e, F[0], F[1]);
+            stp(sGeo, nf, 3, e, F[2], F[3]);
+        }
     }
 };
 
@@ -523,9 +552,10 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
                 umin[v] = fmin(umin[v], un[v]);
                 umax[v] = fmax(umax[v], un[v]);
             }
-            // this cell's own centre-to-face vector: one pair of loads at the side's offset
-            ro[k][0] = sGeo[(isL ? 4 : 6) * nfl + e];
-            ro[k][1] = sGeo[(isL ? 5 : 7) * nfl + e];
+            // this cell's own centre-to-face vector: one pair, at its side's plane
+            const auto rr = ldp(sGeo, nfl, isL ? 2 : 3, e);
+            ro[k][0] = rr.x;
+            ro[k][1] = rr.y;
             if (s.time_mode != TM_FIXED) lam += wave(cu, cv, ca, g);
         }
         T e2 = T(0);
@@ -624,14 +654,14 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
             T FA[4], FB[4];
             A.flux(s.gma, FA);
             Bq.flux(s.gma, FB);
-            A.store(sGeoW, nf, FA);
-            if (eB != e) Bq.store(sGeoW, nf, FB);
+            A.template store<COMP>(sGeoW, nf, FA);
+            if (eB != e) Bq.template store<COMP>(sGeoW, nf, FB);
         } else {
             FaceIn<T> A;
             A.load(sU, sG, NL, sGeo, sMeta, nf, e);
             T FA[4];
             A.flux(s.gma, FA);
-            A.store(sGeoW, nf, FA);
+            A.template store<COMP>(sGeoW, nf, FA);
         }
     }
     compute_sync(NT);
@@ -654,22 +684,23 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
             if (cs[k] < 0) continue;
             const bool isL = (cs[k] & 1) == 0;
             const int e = cs[k] >> 1;
-            T gnx, gny, Af;
-            lds_geo3(sGeo, nf, e, gnx, gny, Af);
+            const auto F01 = ldp(sGeo, nf, 2, e), F23 = ldp(sGeo, nf, 3, e);
+            const T Fk[4] = {F01.x, F01.y, F23.x, F23.y};
+            T Af = T(0);
+            if constexpr (!COMP) Af = lds_area(sGeo, nf, e);
 #pragma unroll
             for (int v = 0; v < 4; v++) {                        // Flux.cpp:39-42
-                const T Fv = sGeo[(3 + v) * nf + e];
-                if constexpr (COMP) {
-                    const T x = isL ? -(Af * Fv) : Af * Fv;
-                    two_sum(R[v], Rc[v], x);
+                const T Fv = Fk[v];
+                if constexpr (COMP) {                            // Fv holds A_f F here
+                    two_sum(R[v], Rc[v], isL ? -Fv : Fv);
                 } else {
                     if (isL) R[v] -= Af * Fv;
                     else     R[v] += Af * Fv;
                 }
             }
-            if (s.time_mode == TM_LOCAL) {
+            if (s.time_mode == TM_LOCAL) {                       // the normal only for the local dt
                 FaceGeo<T> g;
-                g.nx = gnx; g.ny = gny; g.Af = Af;
+                lds_geo3(sGeo, nf, e, g.nx, g.ny, g.Af);
                 lam += wave(cu, cv, ca, g);
             }
         }
@@ -720,8 +751,8 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
     if constexpr (!ARENA) finish_step(s, r2, bad, dt_used);
 }
 
-// Face records in tile order, component-major per tile: for tile t with entries
-// [f0, f0 + nf), component k of entry e is tgeo[8 f0 + k nf + e] (zeros for padding).
+// Face records in tile order, pair-major per tile: for tile t with entries [f0, f0 + nf),
+// component k of entry e is tgeo[8 f0 + 2 ((k / 2) nf + e) + k % 2] (zeros for padding).
 template <class T>
 __global__ void gather_geo_kernel(int ntiles, const int* __restrict__ foff, const int* __restrict__ efid,
                                   const FaceGeo<double>* __restrict__ geo, T* __restrict__ tgeo) {
@@ -737,7 +768,7 @@ __global__ void gather_geo_kernel(int ntiles, const int* __restrict__ foff, cons
             c[0] = g.nx; c[1] = g.ny; c[2] = g.Af; c[3] = g.If; c[4] = g.rLx; c[5] = g.rLy; c[6] = g.rRx; c[7] = g.rRy;
         }
 #pragma unroll
-        for (int k = 0; k < 8; k++) out[k * nf + e] = T(c[k]);
+        for (int j = 0; j < 4; j++) stp(out, nf, j, e, T(c[2 * j]), T(c[2 * j + 1]));
     }
 }
 

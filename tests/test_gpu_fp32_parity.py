@@ -24,9 +24,9 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 EPS32 = 2.0 ** -23
-STATE_ULPS = 8
-DT_ULPS = 8
-RES_ULPS = 4096
+STATE_ULPS = 4
+DT_ULPS = 4
+RES_ULPS = 4
 
 STEPS = 30
 
