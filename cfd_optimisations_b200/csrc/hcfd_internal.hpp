@@ -42,9 +42,13 @@ struct TilePlan {
 // Internal cell order: cells sorted by the Morton key of their vertex-average centre.
 // Returns perm with perm[internal] = input index.
 std::vector<int> morton_order(const hcfd_mesh_view& v);
+// face_groups: number each tile's face entries so that every run of 8 consecutive entries
+// reads cells in distinct shared-memory bank groups on each side where it can (the entry
+// order pass 2's face phase reads in); pass 1, which reads entries through its cells' slots,
+// keeps the order in which its cells meet their faces.
 int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, const std::vector<int>& cf_con,
                     const std::vector<char>& ghost, const std::vector<int>& perm, int F_BC,
-                    const std::vector<int>& bc_first, int B, int W, TilePlan& P);
+                    const std::vector<int>& bc_first, int B, int W, TilePlan& P, bool face_groups = false);
 }  // namespace hcfd
 
 namespace hcfd {

@@ -31,6 +31,65 @@ unsigned long long spread16(unsigned long long x) {
 }
 }  // namespace
 
+// Renumbers the real (non-padding) entries [e0, e0 + n) of tile t for pass 2's face phase,
+// in which the 8 lanes of a quarter warp read the 16-byte cell and gradient chunks of 8
+// consecutive entries' left cells, then of their right cells.  Those reads conflict in shared
+// memory when two lanes read different cells of the same bank group (local cell index mod 8,
+// every plane being a multiple of 128 bytes apart).  Entries are taken greedily into groups of
+// 8: each pick comes from the non-empty (left mod 8, right mod 8) class that adds the fewest
+// conflicts to the group (a cell already read in the group adds none), the fullest class first
+// among equals.  Only the numbering changes: each cell's slots still list its faces in
+// increasing face order, so every per-cell sum keeps its order.
+static void group_entries(TilePlan& P, int t, int e0, int n, int nb) {
+    if (n <= 8) return;
+    std::vector<int> bucket_head[64];
+    for (int e = 0; e < n; e++) {
+        const short* m = &P.meta[4 * (size_t) (e0 + e)];
+        bucket_head[(m[0] & 7) * 8 + (m[1] & 7)].push_back(e);
+    }
+    int pos[64] = {0};
+    std::vector<int> order;
+    order.reserve(n);
+    while ((int) order.size() < n) {
+        int ua[8], ub[8];
+        for (int k = 0; k < 8; k++) ua[k] = ub[k] = -1;
+        const int g = std::min(8, n - (int) order.size());
+        for (int i = 0; i < g; i++) {
+            int best = -1, bcost = 3, bleft = 0;
+            for (int k = 0; k < 64; k++) {
+                const int left = (int) bucket_head[k].size() - pos[k];
+                if (left <= 0) continue;
+                const short* m = &P.meta[4 * (size_t) (e0 + bucket_head[k][pos[k]])];
+                const int a = m[0], b = m[1];
+                const int cost = (ua[a & 7] >= 0 && ua[a & 7] != a) + (ub[b & 7] >= 0 && ub[b & 7] != b);
+                if (cost < bcost || (cost == bcost && left > bleft)) { best = k; bcost = cost; bleft = left; }
+            }
+            const int e = bucket_head[best][pos[best]++];
+            const short* m = &P.meta[4 * (size_t) (e0 + e)];
+            if (ua[m[0] & 7] < 0) ua[m[0] & 7] = m[0];
+            if (ub[m[1] & 7] < 0) ub[m[1] & 7] = m[1];
+            order.push_back(e);
+        }
+    }
+    std::vector<int> newpos(n);
+    std::vector<int> efid(n);
+    std::vector<short> meta(4 * (size_t) n);
+    for (int i = 0; i < n; i++) {
+        const int e = order[i];
+        newpos[e] = i;
+        efid[i] = P.efid[e0 + e];
+        for (int k = 0; k < 4; k++) meta[4 * (size_t) i + k] = P.meta[4 * (size_t) (e0 + e) + k];
+    }
+    std::copy(efid.begin(), efid.end(), P.efid.begin() + e0);
+    std::copy(meta.begin(), meta.end(), P.meta.begin() + 4 * (size_t) e0);
+    short* cs = &P.cslot[(size_t) t * P.B * P.Wp];
+    for (int c = 0; c < nb; c++)
+        for (int k = 0; k < P.Wp; k++) {
+            short& x = cs[(size_t) c * P.Wp + k];
+            if (x >= 0) x = (short) ((newpos[x >> 1] << 1) | (x & 1));
+        }
+}
+
 std::vector<int> morton_order(const hcfd_mesh_view& v) {
     double lo[2] = {1e300, 1e300}, hi[2] = {-1e300, -1e300};
     for (int i = 0; i < v.Nn; i++)
@@ -57,7 +116,7 @@ std::vector<int> morton_order(const hcfd_mesh_view& v) {
 
 int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, const std::vector<int>& cf_con,
                     const std::vector<char>& ghost, const std::vector<int>& perm, int F_BC,
-                    const std::vector<int>& bc_first, int B, int W, TilePlan& P) {
+                    const std::vector<int>& bc_first, int B, int W, TilePlan& P, bool face_groups) {
     const int Nc = v.Nc;
     P.B = B;
     P.W = W;
@@ -112,6 +171,7 @@ int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, con
                 P.cslot[((size_t) t * B + c) * P.Wp + k] = (short) ((e << 1) | (uR == u ? 1 : 0));
             }
         }
+        if (face_groups) group_entries(P, t, e0, (int) P.efid.size() - e0, nb);
         // pad the entries to a multiple of 4 so every per-tile block is a multiple of 16 B
         while (((int) P.efid.size() - e0) % 4) {
             short m[4] = {0, 0, -1, 0};
@@ -153,10 +213,13 @@ extern "C" int hcfd_plan_check(const hcfd_mesh_view* v, int tile, int keep_numbe
     std::vector<int> bc_first;
     for (int col = v->Ncol - v->NBCcol; col < v->Ncol; col++) bc_first.push_back(v->coloff[col]);
     const int B = tile ? tile : 256;
-    TilePlan P;
-    rc = build_tile_plan(*v, cf_off, cf_con, ghost, perm, F_BC, bc_first, B, W, P);
-    if (rc != HCFD_OK) return rc;
     std::vector<int> iperm(Nc);
+    // both entry orders: as the cells meet their faces (pass 1, the arena) and grouped for
+    // pass 2's face phase; info describes the first
+    for (int grouped = 1; grouped >= 0; grouped--) {
+    TilePlan P;
+    rc = build_tile_plan(*v, cf_off, cf_con, ghost, perm, F_BC, bc_first, B, W, P, grouped != 0);
+    if (rc != HCFD_OK) return rc;
     for (int i = 0; i < Nc; i++) iperm[perm[i]] = i;
     auto bad = [&](const char* what, int t) {
         return fail(HCFD_EINVAL, std::string("plan_check: ") + what + " (tile " + std::to_string(t) + ")");
@@ -225,9 +288,10 @@ extern "C" int hcfd_plan_check(const hcfd_mesh_view* v, int tile, int keep_numbe
             }
         }
     }
-    if (info) {
+    if (info && !grouped) {
         info[0] = P.ntiles; info[1] = P.Hmax; info[2] = P.Fmax; info[3] = E;
         info[4] = internal; info[5] = cut; info[6] = W; info[7] = (long long) P.halo.size();
+    }
     }
     return HCFD_OK;
 }

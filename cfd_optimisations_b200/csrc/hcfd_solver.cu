@@ -422,7 +422,8 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
                 if (need(s->tp[0].plan, true) <= (size_t) maxsm) { s->split = false; ok = true; break; }
                 continue;
             }
-            rc = hcfd::build_tile_plan(*mv, cf_off, cf_con, ghost, perm, s->F_BC, bc_first, t, s->W, s->tp[1].plan);
+            rc = hcfd::build_tile_plan(*mv, cf_off, cf_con, ghost, perm, s->F_BC, bc_first, t, s->W, s->tp[1].plan,
+                                       true);
             if (rc != HCFD_OK) return rc;
             if (need(s->tp[1].plan, true) <= (size_t) maxsm) {
                 s->split = true;
