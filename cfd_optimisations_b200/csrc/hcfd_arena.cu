@@ -225,7 +225,7 @@ struct hcfd_arena {
     void* iv = nullptr;
     short* cslot = nullptr;
     void* tgeo = nullptr;
-    short* tmeta = nullptr;
+    unsigned* tmeta = nullptr;              // pack_meta words
     int* halo = nullptr;
     double* inst_dt = nullptr;
     unsigned long long* inst_dtmin = nullptr;
@@ -300,6 +300,7 @@ hcfd::TileArgs<T> arena_args(hcfd_arena* A, int cur, int par) {
     s.freeze_after = A->prm.freeze_limiter_after;
     a.inst_stats = A->stats;
     a.tgeo = (const T*) A->tgeo;
+    a.rec = 8;                             // one plan serves both passes: pass 1 reads If
     a.tmeta = A->tmeta;
     a.halo = A->halo;
     a.cslot = A->cslot;
@@ -514,7 +515,7 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
         (rc = dalloc((char**) &h->phiG, 8 * ts * C)) || (rc = dalloc((char**) &h->iv, ts * C)) ||
         (p.freeze_limiter_after > 0 && (rc = dalloc((char**) &h->phiF, 4 * ts * C))) ||
         (rc = dalloc(&h->cslot, h->Wp * C)) || (rc = dalloc((char**) &h->tgeo, 8 * ts * h->Ecap)) ||
-        (rc = dalloc(&h->tmeta, 4 * h->Ecap)) || (rc = dalloc(&h->halo, h->HLcap)) ||
+        (rc = dalloc(&h->tmeta, h->Ecap)) || (rc = dalloc(&h->halo, h->HLcap)) ||
         (rc = dalloc(&h->inst_dt, p.max_instances)) || (rc = dalloc(&h->inst_dtmin, 2 * (size_t) p.max_instances)) ||
         (rc = dalloc(&h->inst_bc, p.max_instances)) || (rc = dalloc(&h->stats, p.max_instances)) ||
         (rc = dalloc(&h->tiles, 2 * h->tiles_cap)) || (rc = dalloc(&h->act, p.max_instances)) ||
@@ -674,7 +675,8 @@ int hcfd_arena_admit_prepared(hcfd_arena* A, const hcfd_admission* D, int* slot_
     up(d_halo, P.halo.data(), 4 * I.nh);
     up(d_nodes, mv->nodes, 16 * (size_t) mv->Nn);
     up(I.d_perm, D->perm.data(), 4 * (size_t) Nc);
-    up(A->tmeta + 4 * I.e0, P.meta.data(), 2 * P.meta.size());
+    const std::vector<unsigned> mw = hcfd::packed_meta(P);
+    up(A->tmeta + I.e0, mw.data(), 4 * mw.size());
     up(A->cslot + A->Wp * I.c0, P.cslot.data(), 2 * P.cslot.size());
     if (ce == cudaSuccess) {
         arena_cellmap_kernel<<<nblk(2 * (long long) Nf, 256), 256, 0, st>>>(2 * (long long) Nf, (int) I.c0, d_iperm, d_fcu, d_fcg);
@@ -685,10 +687,10 @@ int hcfd_arena_admit_prepared(hcfd_arena* A, const hcfd_admission* D, int* slot_
         ce = cudaMemsetAsync((char*) A->iv + A->tsz * I.c0, 0, A->tsz * I.ncell, st);
         if (A->fp32()) {
             arena_iv_kernel<float><<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_ivu, I.d_perm, (float*) A->iv + I.c0);
-            hcfd::gather_geo_kernel<float><<<P.ntiles, 128, 0, st>>>(P.ntiles, d_foff, d_efid, d_geo, (float*) A->tgeo + 8 * I.e0);
+            hcfd::gather_geo_kernel<float><<<P.ntiles, 128, 0, st>>>(P.ntiles, d_foff, d_efid, d_geo, (float*) A->tgeo + 8 * I.e0, 8);
         } else {
             arena_iv_kernel<double><<<nblk(Nc, 256), 256, 0, st>>>(Nc, d_ivu, I.d_perm, (double*) A->iv + I.c0);
-            hcfd::gather_geo_kernel<double><<<P.ntiles, 128, 0, st>>>(P.ntiles, d_foff, d_efid, d_geo, (double*) A->tgeo + 8 * I.e0);
+            hcfd::gather_geo_kernel<double><<<P.ntiles, 128, 0, st>>>(P.ntiles, d_foff, d_efid, d_geo, (double*) A->tgeo + 8 * I.e0, 8);
         }
         // initial state into the current buffer, then the ghost cells from the BCs
         const double* u = D->u0;

@@ -182,7 +182,7 @@ int build_tile_plan(const hcfd_mesh_view& v, const std::vector<int>& cf_off, con
         P.hoff[t + 1] = (int) P.halo.size();
         P.Hmax = std::max(P.Hmax, (int) P.halo.size() - h0);
         P.Fmax = std::max(P.Fmax, (int) P.efid.size() - e0);
-        if (B + P.Hmax > 32767) return fail(HCFD_EINVAL, "tile plan: halo too large");
+        if (B + P.Hmax > 8191) return fail(HCFD_EINVAL, "tile plan: halo too large");
     }
     return HCFD_OK;
 }

@@ -59,11 +59,12 @@ void prim_to_cons(const double* q, double gma, double* u) {
 struct TiledPass {
     hcfd::TilePlan plan;
     void* d_tgeo = nullptr;              // face records [entries], T
-    short* d_tmeta = nullptr;
+    unsigned* d_tmeta = nullptr;         // pack_meta words [entries]
     int *d_foff = nullptr, *d_hoff = nullptr, *d_halo = nullptr;
     short* d_cslot = nullptr;
     int* d_efid = nullptr;               // set-up only
     int block = 0;                       // compute threads per CTA
+    int rec = 8;                         // values per face record (7: pass 2 on a plan of its own)
 };
 
 struct hcfd_solver {
@@ -181,6 +182,7 @@ hcfd::TileArgs<T> tile_args(hcfd_solver* s, int time_mode, double dt_or_cfl, con
     hcfd::TileArgs<T> a;
     a.s = step_args<T>(s, time_mode, dt_or_cfl);
     a.tgeo = (const T*) P.d_tgeo;
+    a.rec = P.rec;
     a.tmeta = P.d_tmeta;
     a.foff = P.d_foff;
     a.hoff = P.d_hoff;
@@ -492,7 +494,8 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         for (int k = 0; k < (h->split ? 2 : 1); k++) {
             TiledPass& P = h->tp[k];
             const size_t E = P.plan.efid.size();
-            if ((rc = dalloc((char**) &P.d_tgeo, tsz * 8 * E)) || (rc = dalloc(&P.d_tmeta, 4 * E)) ||
+            P.rec = k == 1 ? 7 : 8;     // pass 2's own plan leaves out If, which only pass 1 reads
+            if ((rc = dalloc((char**) &P.d_tgeo, tsz * P.rec * E)) || (rc = dalloc(&P.d_tmeta, E)) ||
                 (rc = dalloc(&P.d_foff, P.plan.foff.size())) || (rc = dalloc(&P.d_hoff, P.plan.hoff.size())) ||
                 (rc = dalloc(&P.d_halo, P.plan.halo.size())) || (rc = dalloc(&P.d_cslot, P.plan.cslot.size())) ||
                 (rc = dalloc(&P.d_efid, E))) {
@@ -524,7 +527,8 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         for (int k = 0; k < (h->split ? 2 : 1); k++) {
             TiledPass& T = h->tp[k];
             const hcfd::TilePlan& P = T.plan;
-            if (ce == cudaSuccess) ce = up(T.d_tmeta, P.meta.data(), 2 * P.meta.size());
+            const std::vector<unsigned> mw = hcfd::packed_meta(P);
+            if (ce == cudaSuccess) ce = up(T.d_tmeta, mw.data(), 4 * mw.size());
             if (ce == cudaSuccess) ce = up(T.d_foff, P.foff.data(), 4 * P.foff.size());
             if (ce == cudaSuccess) ce = up(T.d_hoff, P.hoff.data(), 4 * P.hoff.size());
             if (ce == cudaSuccess) ce = up(T.d_halo, P.halo.data(), 4 * P.halo.size());
@@ -548,8 +552,8 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
             TiledPass& T = h->tp[k];
             const int nt = T.plan.ntiles;
             if (T.plan.efid.empty()) continue;
-            if (f32) hcfd::gather_geo_kernel<float><<<nt, 128, 0, st>>>(nt, T.d_foff, T.d_efid, h->d_geo64, (float*) T.d_tgeo);
-            else hcfd::gather_geo_kernel<double><<<nt, 128, 0, st>>>(nt, T.d_foff, T.d_efid, h->d_geo64, (double*) T.d_tgeo);
+            if (f32) hcfd::gather_geo_kernel<float><<<nt, 128, 0, st>>>(nt, T.d_foff, T.d_efid, h->d_geo64, (float*) T.d_tgeo, T.rec);
+            else hcfd::gather_geo_kernel<double><<<nt, 128, 0, st>>>(nt, T.d_foff, T.d_efid, h->d_geo64, (double*) T.d_tgeo, T.rec);
         }
         if (!h->tiled && f32)
             hcfd::convert_geo_kernel<float><<<nblk(Nf, 256), 256, 0, st>>>(Nf, h->d_geo64, (hcfd::FaceGeo<float>*) h->d_geoT);

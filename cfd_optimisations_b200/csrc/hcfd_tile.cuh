@@ -12,15 +12,19 @@
 // The arithmetic is that of the thread-per-cell kernels in hcfd_kernels.cuh, operation for
 // operation; only where the operands come from differs.
 #pragma once
+#include "hcfd_internal.hpp"
 #include "hcfd_kernels.cuh"
+
+#include <vector>
 
 namespace hcfd {
 
 template <class T>
 struct TileArgs {
     StepArgs<T> s;                         // state, stats, BC table, modes
-    const T* __restrict__ tgeo;            // face records, per tile pair-major: [4][nf] pairs
-    const short* __restrict__ tmeta;       // 4 shorts per entry: la, lb, bc, 0
+    const T* __restrict__ tgeo;            // face records, per tile pair-major (see ldp), rec values each
+    int rec;                               // values per face record: 8, or 7 in a pass-2 plan of its own
+    const unsigned* __restrict__ tmeta;    // one word per entry (pack_meta): la, lb, bc
     const int* __restrict__ foff;          // [ntiles + 1], multiples of 4
     const int* __restrict__ hoff;          // [ntiles + 1]
     const int* __restrict__ halo;          // internal cell ids
@@ -43,6 +47,22 @@ struct TileArgs {
     int* tile_bad;                         // same layout: a NaN/Inf appeared
     int par;                               // which dtmin slot this step uses
 };
+
+// Metadata of a face entry in one 32-bit word: the local index (tile cell 0..B-1, halo cell
+// B..) of its left cell in bits 0-12, of its right cell in bits 13-25, and its boundary
+// condition's index + 1 in bits 26-30 (0: an interior face).  The plan keeps B + halo below
+// 8192 and at most 16 boundary conditions.
+__host__ __device__ __forceinline__ unsigned pack_meta(int la, int lb, int bc) {
+    return (unsigned) la | ((unsigned) lb << 13) | ((unsigned) (bc + 1) << 26);
+}
+inline std::vector<unsigned> packed_meta(const TilePlan& P) {
+    std::vector<unsigned> w(P.meta.size() / 4);
+    for (size_t i = 0; i < w.size(); i++) w[i] = pack_meta(P.meta[4 * i], P.meta[4 * i + 1], P.meta[4 * i + 2]);
+    return w;
+}
+__device__ __forceinline__ int meta_la(unsigned w) { return (int) (w & 0x1FFFu); }
+__device__ __forceinline__ int meta_lb(unsigned w) { return (int) ((w >> 13) & 0x1FFFu); }
+__device__ __forceinline__ int meta_bc(unsigned w) { return (int) (w >> 26) - 1; }
 
 // Cells, face entries and halo of tile t (single mesh) or of active tile t (arena).
 template <bool ARENA, class T>
@@ -179,9 +199,15 @@ __device__ __forceinline__ void stp(T* p, int nf, int j, int e, T x, T y) {
     v.x = x; v.y = y;
     reinterpret_cast<typename PairOf<T>::type*>(p)[j * nf + e] = v;
 }
-// The length A_f alone (first half of pair 1).
+// Records of 8 values (pass 1, and pass 2 when it shares pass 1's plan, the arena's too):
+// pairs (nx, ny), (Af, If), (rLx, rLy), (rRx, rRy).  Records of 7 values (pass 2 on a plan of
+// its own, which never reads If): pairs (nx, ny), (rLx, rLy), (rRx, rRy), then Af alone in a
+// plane of scalars.  rplane gives the pair plane of rL (rR follows it).
+__device__ __forceinline__ int rplane(int rec) { return rec == 7 ? 1 : 2; }
 template <class T>
-__device__ __forceinline__ T lds_area(const T* p, int nf, int e) { return p[2 * (nf + e)]; }
+__device__ __forceinline__ T lds_area(const T* p, int nf, int e, int rec) {
+    return rec == 7 ? p[6 * nf + e] : p[2 * (nf + e)];
+}
 
 template <class T>
 __device__ __forceinline__ void lds_geo(const T* p, int nf, int e, FaceGeo<T>& g) {
@@ -198,9 +224,9 @@ __device__ __forceinline__ void lds_geo4(const T* p, int nf, int e, FaceGeo<T>& 
 
 // Normal and length only (the components pass 2's flux write leaves intact).
 template <class T>
-__device__ __forceinline__ void lds_geo3(const T* p, int nf, int e, T& nx, T& ny, T& Af) {
+__device__ __forceinline__ void lds_geo3(const T* p, int nf, int e, int rec, T& nx, T& ny, T& Af) {
     const auto a = ldp(p, nf, 0, e);
-    nx = a.x; ny = a.y; Af = lds_area(p, nf, e);
+    nx = a.x; ny = a.y; Af = lds_area(p, nf, e, rec);
 }
 
 __host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~size_t(127); }
@@ -218,7 +244,7 @@ struct TileSmem {
         u = p;     p += align128((size_t) (B + Hmax) * sizeof(Cell4<T>));
         g = p;     if (pass2) p += align128((size_t) (B + Hmax) * sizeof(Grad8<T>));
         geo = p;   p += align128((size_t) Fmax * sizeof(FaceGeo<T>));
-        meta = p;  p += align128((size_t) Fmax * 8);
+        meta = p;  p += align128((size_t) Fmax * 4);
         cslot = p; p += align128((size_t) B * Wp * sizeof(short));
         iv = p;    p += align128((size_t) B * sizeof(T));
         stage = p;
@@ -290,7 +316,7 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
         Grad8<T>* sG = reinterpret_cast<Grad8<T>*>(st + L.g);
         if (lane == 0) {
             const unsigned bu = nb * sizeof(Cell4<T>), bg = PASS2 ? nb * sizeof(Grad8<T>) : 0u;
-            const unsigned bf = nf * sizeof(FaceGeo<T>), bm = nf * 8u;
+            const unsigned bf = nf * a.rec * (unsigned) sizeof(T), bm = nf * 4u;
             const unsigned bs = a.B * a.Wp * sizeof(short), bi = a.B * sizeof(T);
             // the tile's descriptor and instance scalars, published by the release of the
             // arrive below
@@ -314,8 +340,8 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
                              full + buf);
             }
             if (bf) {
-                bulk_g2s(st + L.geo, a.tgeo + (size_t) f0 * 8, bf, full + buf);
-                bulk_g2s(st + L.meta, a.tmeta + (size_t) f0 * 4, bm, full + buf);
+                bulk_g2s(st + L.geo, a.tgeo + (size_t) f0 * a.rec, bf, full + buf);
+                bulk_g2s(st + L.meta, a.tmeta + f0, bm, full + buf);
             }
             bulk_g2s(st + L.cslot, a.cslot + (size_t) base * a.Wp, bs, full + buf);
             bulk_g2s(st + L.iv, a.s.iv + base, bi, full + buf);
@@ -413,17 +439,22 @@ struct FaceIn {
     T uoL[4], uqR[4], nx, ny, Af;
     int e;
     __device__ __forceinline__ void load(const Cell4<T>* sU, const Grad8<T>* sG, int NL, const T* sGeo,
-                                         const short* sMeta, int nf, int e_) {
+                                         const unsigned* sMeta, int nf, int rec, int e_) {
         e = e_;
-        const short4 m = *reinterpret_cast<const short4*>(sMeta + 4 * e);
-        const int bc = m.z;
+        const unsigned w = sMeta[e];
+        const int bc = meta_bc(w);
+        const int mx = meta_la(w), my = meta_lb(w);
+        const int rp = rplane(rec);
         FaceGeo<T> g;
-        lds_geo(sGeo, nf, e, g);
-        nx = g.nx; ny = g.ny; Af = g.Af;
+        {
+            const auto n2 = ldp(sGeo, nf, 0, e), rl = ldp(sGeo, nf, rp, e), rr = ldp(sGeo, nf, rp + 1, e);
+            g.nx = n2.x; g.ny = n2.y; g.rLx = rl.x; g.rLy = rl.y; g.rRx = rr.x; g.rRy = rr.y;
+        }
+        nx = g.nx; ny = g.ny; Af = lds_area(sGeo, nf, e, rec);
         T uL[4], uR[4], gL[8];
-        lds_cell(sU, NL, m.x, uL);
-        lds_cell(sU, NL, m.y, uR);
-        lds_grad(sG, NL, m.x, gL);
+        lds_cell(sU, NL, mx, uL);
+        lds_cell(sU, NL, my, uR);
+        lds_grad(sG, NL, mx, gL);
         if (bc >= 0) {
             // Ghost on the right: -grad and the same phi as the interior cell with r_R = -r_L
             // (BoundaryConditions/Base.cpp:29-53, Domain.cpp:84-88): the same increment.
@@ -435,7 +466,7 @@ struct FaceIn {
             }
         } else {
             T gR[8];
-            lds_grad(sG, NL, m.y, gR);
+            lds_grad(sG, NL, my, gR);
 #pragma unroll
             for (int v = 0; v < 4; v++) {
                 uoL[v] = uL[v] + (gL[2 * v] * g.rLx + gL[2 * v + 1] * g.rLy);
@@ -444,18 +475,19 @@ struct FaceIn {
         }
     }
     __device__ __forceinline__ void flux(T gma, T F[4]) const { rusanov(uoL, uqR, nx, ny, gma, F); }
-    // F over pairs 2 and 3 (the r vectors) of this entry's staged record: only this thread
-    // reads them in pass 2, and it has read them already.  With AF the product A_f F is stored
-    // instead (the compensated FP32 sums round that product before adding it, so forming it
-    // once per face gives the same bits as forming it in each of the two cells).
+    // F over the two r pairs of this entry's staged record: only this thread reads them in
+    // pass 2, and it has read them already.  With AF the product A_f F is stored instead (the
+    // compensated FP32 sums round that product before adding it, so forming it once per face
+    // gives the same bits as forming it in each of the two cells).
     template <bool AF>
-    __device__ __forceinline__ void store(T* sGeo, int nf, const T F[4]) const {
+    __device__ __forceinline__ void store(T* sGeo, int nf, int rec, const T F[4]) const {
+        const int rp = rplane(rec);
         if (AF) {
-            stp(sGeo, nf, 2, e, F[0] * Af, F[1] * Af);
-            stp(sGeo, nf, 3, e, F[2] * Af, F[3] * Af);
+            stp(sGeo, nf, rp, e, F[0] * Af, F[1] * Af);
+            stp(sGeo, nf, rp + 1, e, F[2] * Af, F[3] * Af);
         } else {
-            stp(sGeo, nf, 2, e, F[0], F[1]);
-            stp(sGeo, nf, 3, e, F[2], F[3]);
+            stp(sGeo, nf, rp, e, F[0], F[1]);
+            stp(sGeo, nf, rp + 1, e, F[2], F[3]);
         }
     }
 };
@@ -499,7 +531,7 @@ struct FaceIn {
         const Cell4<T>* sU = reinterpret_cast<const Cell4<T>*>(st + L.u);                        \
         const T* sGeo = reinterpret_cast<const T*>(st + L.geo);                                  \
         const int nfl = si.nf;                                                                   \
-        const short* sMeta = reinterpret_cast<const short*>(st + L.meta);                        \
+        const unsigned* sMeta = reinterpret_cast<const unsigned*>(st + L.meta);                  \
         const short* sSlot = reinterpret_cast<const short*>(st + L.cslot);                       \
         const T* sIv = reinterpret_cast<const T*>(st + L.iv);
 
@@ -537,7 +569,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
             const bool isL = (cs[k] & 1) == 0;
             FaceGeo<T> g;
             lds_geo4(sGeo, nfl, e, g);
-            const int nbl = sMeta[4 * e + (isL ? 1 : 0)];
+            const int nbl = isL ? meta_lb(sMeta[e]) : meta_la(sMeta[e]);
             T un[4];
             lds_cell(sU, NL, nbl, un);
 #pragma unroll
@@ -649,19 +681,19 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
         if (sizeof(T) == 4 || (int) (threadIdx.x & ~31u) < pairs) {
             const int eB = (e + NT < nf) ? e + NT : e;
             FaceIn<T> A, Bq;
-            A.load(sU, sG, NL, sGeo, sMeta, nf, e);
-            Bq.load(sU, sG, NL, sGeo, sMeta, nf, eB);
+            A.load(sU, sG, NL, sGeo, sMeta, nf, a.rec, e);
+            Bq.load(sU, sG, NL, sGeo, sMeta, nf, a.rec, eB);
             T FA[4], FB[4];
             A.flux(s.gma, FA);
             Bq.flux(s.gma, FB);
-            A.template store<COMP>(sGeoW, nf, FA);
-            if (eB != e) Bq.template store<COMP>(sGeoW, nf, FB);
+            A.template store<COMP>(sGeoW, nf, a.rec, FA);
+            if (eB != e) Bq.template store<COMP>(sGeoW, nf, a.rec, FB);
         } else {
             FaceIn<T> A;
-            A.load(sU, sG, NL, sGeo, sMeta, nf, e);
+            A.load(sU, sG, NL, sGeo, sMeta, nf, a.rec, e);
             T FA[4];
             A.flux(s.gma, FA);
-            A.template store<COMP>(sGeoW, nf, FA);
+            A.template store<COMP>(sGeoW, nf, a.rec, FA);
         }
     }
     compute_sync(NT);
@@ -684,10 +716,11 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
             if (cs[k] < 0) continue;
             const bool isL = (cs[k] & 1) == 0;
             const int e = cs[k] >> 1;
-            const auto F01 = ldp(sGeo, nf, 2, e), F23 = ldp(sGeo, nf, 3, e);
+            const int rp = rplane(a.rec);
+            const auto F01 = ldp(sGeo, nf, rp, e), F23 = ldp(sGeo, nf, rp + 1, e);
             const T Fk[4] = {F01.x, F01.y, F23.x, F23.y};
             T Af = T(0);
-            if constexpr (!COMP) Af = lds_area(sGeo, nf, e);
+            if constexpr (!COMP) Af = lds_area(sGeo, nf, e, a.rec);
 #pragma unroll
             for (int v = 0; v < 4; v++) {                        // Flux.cpp:39-42
                 const T Fv = Fk[v];
@@ -700,7 +733,7 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
             }
             if (s.time_mode == TM_LOCAL) {                       // the normal only for the local dt
                 FaceGeo<T> g;
-                lds_geo3(sGeo, nf, e, g.nx, g.ny, g.Af);
+                lds_geo3(sGeo, nf, e, a.rec, g.nx, g.ny, g.Af);
                 lam += wave(cu, cv, ca, g);
             }
         }
@@ -722,12 +755,13 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
         for (int k = 0; k < W; k++) {
             if (cs[k] < 0 || (cs[k] & 1)) continue;
             const int e = cs[k] >> 1;
-            const int bc = sMeta[4 * e + 2];
+            const unsigned w = sMeta[e];
+            const int bc = meta_bc(w);
             if (bc < 0) continue;
-            const int lb = sMeta[4 * e + 1];
+            const int lb = meta_lb(w);
             const int gi = lb < a.B ? base + lb : __ldg(a.halo + h0t + lb - a.B);
             T gnx, gny, gA;
-            lds_geo3(sGeo, nf, e, gnx, gny, gA);
+            lds_geo3(sGeo, nf, e, a.rec, gnx, gny, gA);
             T ug[4];
             const BCTable* bt = ARENA ? a.inst_bc + inst : &s.bc;
             ghost_state(bt->type[bc], un_, gnx, gny, s.gma, bt->UBC[bc], bt->QBC[bc], ug);
@@ -751,15 +785,15 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
     if constexpr (!ARENA) finish_step(s, r2, bad, dt_used);
 }
 
-// Face records in tile order, pair-major per tile: for tile t with entries [f0, f0 + nf),
-// component k of entry e is tgeo[8 f0 + 2 ((k / 2) nf + e) + k % 2] (zeros for padding).
+// Face records in tile order, pair-major per tile, rec values each (8 or 7; see rplane):
+// tile t with entries [f0, f0 + nf) starts at tgeo[rec f0] (zeros for padding).
 template <class T>
 __global__ void gather_geo_kernel(int ntiles, const int* __restrict__ foff, const int* __restrict__ efid,
-                                  const FaceGeo<double>* __restrict__ geo, T* __restrict__ tgeo) {
+                                  const FaceGeo<double>* __restrict__ geo, T* __restrict__ tgeo, int rec) {
     const int t = blockIdx.x;
     if (t >= ntiles) return;
     const int f0 = foff[t], nf = foff[t + 1] - f0;
-    T* out = tgeo + (size_t) 8 * f0;
+    T* out = tgeo + (size_t) rec * f0;
     for (int e = threadIdx.x; e < nf; e += blockDim.x) {
         const int f = efid[f0 + e];
         double c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -767,8 +801,15 @@ __global__ void gather_geo_kernel(int ntiles, const int* __restrict__ foff, cons
             const FaceGeo<double> g = geo[f];
             c[0] = g.nx; c[1] = g.ny; c[2] = g.Af; c[3] = g.If; c[4] = g.rLx; c[5] = g.rLy; c[6] = g.rRx; c[7] = g.rRy;
         }
+        if (rec == 7) {
+            stp(out, nf, 0, e, T(c[0]), T(c[1]));
+            stp(out, nf, 1, e, T(c[4]), T(c[5]));
+            stp(out, nf, 2, e, T(c[6]), T(c[7]));
+            out[6 * nf + e] = T(c[2]);
+        } else {
 #pragma unroll
-        for (int j = 0; j < 4; j++) stp(out, nf, j, e, T(c[2 * j]), T(c[2 * j + 1]));
+            for (int j = 0; j < 4; j++) stp(out, nf, j, e, T(c[2 * j]), T(c[2 * j + 1]));
+        }
     }
 }
 

@@ -27,8 +27,12 @@ order) and the stream's sequential service time is estimated from them per cell-
 in the output (the headline ratio).  One rate per cell-step is exact when a step's cost is
 proportional to its cells; with a fixed cost per step as well, it is right only when the
 sample's cell-step-weighted mean size matches the stream's.  A second estimate therefore fits
-a step cost a + b * triangles to the sample and applies it request by request.  The same
-sample gives the served results' errors against FP64.
+a step cost a + b * triangles to the sample and applies it request by request.  A third adds
+each request's own overhead (mesh construction, solver set-up, download: wall time less
+device time on the sample, fitted as c + d * triangles), so that the sequential loop is
+charged what the served latencies include.  The same sample gives the served results' errors
+against FP64.  `run_prefix` (the bench's served leg) runs the sequential loop for real on
+every request of a stream prefix instead.
 """
 from __future__ import annotations
 
@@ -261,12 +265,14 @@ def solve_alone_fp64(r: Request, cfl: float, orders: float, max_steps: int, chun
             return ms, dict(steps=steps, drop=drop_of(st), why=why), s.U()
 
 
-def sequential_service(reqs, steps_by_rid: dict, s_per_step) -> tuple[float, list[float]]:
+def sequential_service(reqs, steps_by_rid: dict, s_per_step, overhead=None) -> tuple[float, list[float]]:
     """Makespan and latencies of serving `reqs` one at a time in arrival order, request r
-    taking steps_by_rid[r.rid] steps of s_per_step(r.triangles) seconds each."""
+    taking steps_by_rid[r.rid] steps of s_per_step(r.triangles) seconds each, plus
+    overhead(r.triangles) seconds when given."""
     t_free, lat = 0.0, []
     for r in reqs:
-        t_free = max(t_free, r.t_arrive) + steps_by_rid[r.rid] * s_per_step(r.triangles)
+        t = steps_by_rid[r.rid] * s_per_step(r.triangles) + (overhead(r.triangles) if overhead else 0.0)
+        t_free = max(t_free, r.t_arrive) + t
         lat.append(t_free - r.t_arrive)
     return t_free, lat
 
@@ -444,7 +450,9 @@ def main():
     for r in reqs:
         if r.rid not in sample:
             continue
+        tw = time.perf_counter()
         ms, info, U64 = solve_alone_fp64(r, a.cfl, a.orders, a.max_steps, a.chunk)
+        info["wall_s"] = time.perf_counter() - tw      # mesh, set-up, steps and download
         base.append((r, ms / 1e3, info))
         served = next(x for x in res if x.rid == r.rid)
         den = np.abs(U64).max(axis=1)
@@ -472,6 +480,19 @@ def main():
     out["fp64_sequential_affine"] = dict(s_per_step_fixed=a0, s_per_cell_step=b0, estimated_makespan_s=t_aff,
                                          solves_per_s=len(reqs) / t_aff, latency_s=percentiles(lat_aff))
     out["speedup_solves_per_s_affine"] = out["served"]["solves_per_s"] / out["fp64_sequential_affine"]["solves_per_s"]
+    # end to end, as the served latencies are measured: each sampled request's wall time (mesh,
+    # solver set-up, steps, download) as device time plus a per-request overhead, the overhead
+    # fitted as c + d * triangles on the sample and charged request by request with the affine
+    # step cost above
+    oh = [max(0.0, i["wall_s"] - s) for _, s, i in base]
+    c0, d0 = affine_step_model([r.triangles for r, _, _ in base], oh)
+    t_e2e, lat_e2e = sequential_service(reqs, steps_by_rid, lambda tri: a0 + b0 * tri,
+                                        overhead=lambda tri: c0 + d0 * tri)
+    out["fp64_sequential_end_to_end"] = dict(overhead_s_fixed=c0, overhead_s_per_triangle=d0,
+                                             sample_wall_s=sum(i["wall_s"] for _, _, i in base),
+                                             estimated_makespan_s=t_e2e, solves_per_s=len(reqs) / t_e2e,
+                                             latency_s=percentiles(lat_e2e))
+    out["speedup_solves_per_s_end_to_end"] = out["served"]["solves_per_s"] / out["fp64_sequential_end_to_end"]["solves_per_s"]
     e32 = [e["rel_linf"] for e in errs]
     out["fp32_vs_fp64_rel_linf"] = dict(n=len(e32), max=max(e32), median=float(np.median(e32)), per_request=errs)
     out["fp64_vs_fp64_initial_density_plus_one_ulp_rel_linf"] = dict(n=len(errs64), max=max(errs64),
