@@ -337,9 +337,9 @@ def main():
     ntri = s.Nreal
     Nc, Nf = s.Nc, s.Nf
     s.step(args.warmup, H.GLOBAL_CFL, CFL)
-    # per-kernel events on every 10th step of the timed region (the events' own gaps stay
-    # out of the other nine)
-    s.profile(True, every=10)
+    # per-kernel events on every 4th step of the timed region (the events' own gaps stay out
+    # of the other three)
+    s.profile(True, every=4)
     barrier(dist)
     H.device_sync()
     with ClockSampler(local) as clk:
