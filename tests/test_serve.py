@@ -180,3 +180,17 @@ def test_sequential_service_and_step_models():
     assert a == pytest.approx(2e-5, rel=1e-6) and b == pytest.approx(1.1e-10, rel=1e-6)
     a, b = serve.affine_step_model(x, 1.1e-10 * x - 1e-6)              # a negative fixed cost is clamped
     assert a == 0.0 and b > 0
+
+
+def test_sequential_service_charges_each_request_its_overhead():
+    """The end-to-end sequential estimate: each request takes its steps plus its own overhead
+    (mesh, set-up, download), one at a time in arrival order."""
+    from cfd_optimisations_b200.serve import Request, sequential_service
+    reqs = [Request(0, 0.0, 11, 6, 2.0, 10.0, 1), Request(1, 0.5, 11, 6, 2.0, 10.0, 2), Request(2, 10.0, 11, 6, 2.0, 10.0, 3)]
+    steps = {0: 100, 1: 100, 2: 100}
+    span, lat = sequential_service(reqs, steps, lambda tri: 0.01, overhead=lambda tri: 0.5)
+    # request 0: 0 -> 1.5; request 1 waits: 1.5 -> 3.0; request 2 arrives at 10: 10 -> 11.5
+    assert span == pytest.approx(11.5)
+    assert lat == pytest.approx([1.5, 2.5, 1.5])
+    span0, _ = sequential_service(reqs, steps, lambda tri: 0.01)
+    assert span0 == pytest.approx(11.0)
