@@ -207,6 +207,20 @@ __device__ __forceinline__ void rusanov(const T UL[4], const T UR[4], T n0, T n1
     for (int v = 0; v < 4; v++) F[v] = T(0.5) * ((FL[v] + FR[v]) - S * (UR[v] - UL[v]));
 }
 
+// Green-Gauss weights of one face seen from one of its cells: the cell's own state weighs
+// ws, its neighbour's wn (If and 1 - If, by side), and the face's contribution enters with
+// the signed length sA (+A_f into the left cell, -A_f into the right one).  One select of
+// two weights per face takes the place of selecting the left and right state of every
+// variable; the product u_CL If + u_CR (1 - If) is the same sum, the two products possibly
+// fused in the other order on the right cell (a rounding-level difference).
+template <class T>
+__device__ __forceinline__ void face_weights(bool isL, T If, T Af, T& ws, T& wn, T& sA) {
+    const T w1 = If, w2 = T(1) - If;
+    ws = isL ? w1 : w2;
+    wn = isL ? w2 : w1;
+    sA = isL ? Af : -Af;
+}
+
 // Spectral-radius term of one face for the local time step: (|u.n| + a) A_f from the
 // cell's own state (u, v, a precomputed).
 template <class T>
@@ -334,16 +348,16 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
                 ld_geo(a.geo, f, g);
                 T un[4];
                 ld_cell(a.U, a.Nc, s[k].y, un);
+                // GaussGreen.cpp:25-28: uf = u_CL If + u_CR (1 - If); +uf Af n into CL,
+                // -uf Af n into CR (the side folded into face_weights).
+                T ws, wn, sA;
+                face_weights(isL, g.If, g.Af, ws, wn, sA);
 #pragma unroll
                 for (int v = 0; v < 4; v++) {
-                    // GaussGreen.cpp:25-28: uf = u_CL If + u_CR (1 - If); +uf Af n into CL,
-                    // -uf Af n into CR.
-                    const T uL = isL ? u[v] : un[v];
-                    const T uR = isL ? un[v] : u[v];
-                    const T uf = uL * g.If + uR * (T(1) - g.If);
-                    const T t = uf * g.Af;
-                    if (isL) { G[v][0] += t * g.nx; G[v][1] += t * g.ny; }
-                    else     { G[v][0] -= t * g.nx; G[v][1] -= t * g.ny; }
+                    const T uf = u[v] * ws + un[v] * wn;
+                    const T t = uf * sA;
+                    G[v][0] += t * g.nx;
+                    G[v][1] += t * g.ny;
                     umin[v] = fmin(umin[v], un[v]);        // Limiter.cpp:31-39
                     umax[v] = fmax(umax[v], un[v]);
                 }

@@ -6,9 +6,9 @@
 //
 // pass 1 (thread per tile cell): Green-Gauss gradient, limiter, CFL dt -> phiG (global).
 // pass 2: face phase (thread per face entry) computes each face flux once per tile and
-//         writes F over the staged face record's If/rL/rRx components (the cell phase does
-//         not read them); cell phase (thread per tile cell) sums A_f F of its faces in
-//         increasing face order, updates the cell and refreshes its ghost cells.
+//         writes F over the staged face record's two r pairs (the cell phase does not read
+//         them); cell phase (thread per tile cell) sums A_f F of its faces in increasing face
+//         order, updates the cell and refreshes its ghost cells.
 // The arithmetic is that of the thread-per-cell kernels in hcfd_kernels.cuh, operation for
 // operation; only where the operands come from differs.
 #pragma once
@@ -572,16 +572,19 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
             const int nbl = isL ? meta_lb(sMeta[e]) : meta_la(sMeta[e]);
             T un[4];
             lds_cell(sU, NL, nbl, un);
+            // GaussGreen.cpp:25-28: uf = u_CL If + u_CR (1 - If), added into CL and taken from
+            // CR.  The side is folded into two weights and a signed length once per face
+            // (face_weights) instead of selecting four left/right states and branching per
+            // variable.
+            T ws, wn, sA;
+            face_weights(isL, g.If, g.Af, ws, wn, sA);
 #pragma unroll
             for (int v = 0; v < 4; v++) {
-                // GaussGreen.cpp:25-28 and Limiter.cpp:31-39
-                const T uL = isL ? u[v] : un[v];
-                const T uR = isL ? un[v] : u[v];
-                const T uf = uL * g.If + uR * (T(1) - g.If);
-                const T tt = uf * g.Af;
-                if (isL) { G[v][0] += tt * g.nx; G[v][1] += tt * g.ny; }
-                else     { G[v][0] -= tt * g.nx; G[v][1] -= tt * g.ny; }
-                umin[v] = fmin(umin[v], un[v]);
+                const T uf = u[v] * ws + un[v] * wn;
+                const T tt = uf * sA;
+                G[v][0] += tt * g.nx;
+                G[v][1] += tt * g.ny;
+                umin[v] = fmin(umin[v], un[v]);                  // Limiter.cpp:31-39
                 umax[v] = fmax(umax[v], un[v]);
             }
             // this cell's own centre-to-face vector: one pair, at its side's plane
