@@ -22,6 +22,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libhcfd_gpu.so")
+LIB_CHECKED = os.path.join(LIBDIR, "libhcfd_gpu_checked.so")
 DRIVER = os.path.join(LIBDIR, "hcfd_wedge_driver")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -52,9 +53,7 @@ def _stale(target, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> str:
-    os.makedirs(LIBDIR, exist_ok=True)
-    objdir = os.path.join(PKG, "_build")
+def _build_lib(lib, objdir, defines, verbose, force, ptxas_info) -> None:
     os.makedirs(objdir, exist_ok=True)
     nv = nvcc()
     objs = []
@@ -62,17 +61,26 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + _deps()):
-            cmd = [nv] + ARCH + NVFLAGS + ["-c", src, "-o", obj]
+            cmd = [nv] + ARCH + NVFLAGS + defines + ["-c", src, "-o", obj]
             if ptxas_info and src.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
-    if force or _stale(LIB, objs):
-        cmd = [nv] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread"]
+    if force or _stale(lib, objs):
+        cmd = [nv] + ARCH + ["-shared", "-o", lib] + objs + ["-lpthread"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+
+
+def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False, checked: bool = True) -> str:
+    """Builds the library, its checked twin (every tile index verified on the device before
+    use; selected at run time with HCFD_LIB=checked) and the C++ driver."""
+    os.makedirs(LIBDIR, exist_ok=True)
+    _build_lib(LIB, os.path.join(PKG, "_build"), [], verbose, force, ptxas_info)
+    if checked:
+        _build_lib(LIB_CHECKED, os.path.join(PKG, "_build", "checked"), ["-DHCFD_CHECKED"], verbose, force, False)
     drv_src = os.path.join(CSRC, "drivers", "wedge_driver.cpp")
     if os.path.exists(drv_src) and (force or _stale(DRIVER, [drv_src, LIB] + _deps())):
         cmd = ["g++", "-O2", "-std=c++17", "-pthread", "-I", INCLUDE, drv_src, "-o", DRIVER,

@@ -309,6 +309,9 @@ hcfd::TileArgs<T> arena_args(hcfd_arena* A, int cur, int par) {
     a.Wp = A->Wp;
     a.Hmax = A->Hcur;
     a.Fmax = A->Fcur;
+    a.nentries = (long long) A->Ecap;
+    a.nhalo = (long long) A->HLcap;
+    a.ncap = (long long) A->Ccap;
     a.err = A->err;
     a.polls = 1u << 22;
     a.skip_tile = -1;
@@ -810,6 +813,7 @@ int hcfd_arena_poll(hcfd_arena* A, int max, int* slots, hcfd_step_stats* stats, 
         k++;
     }
     *n = k;
+    if (err & 4u) return fail(HCFD_EINVAL, "arena, checked build: a tile index was out of range (corrupt tile plan)");
     if (err) return fail(HCFD_ETIMEOUT, "arena: a bounded device wait gave up");
     return HCFD_OK;
 }

@@ -62,6 +62,23 @@ struct StepStats {
     int pad;
 };
 
+// Checked build (HCFD_CHECKED, lib/libhcfd_gpu_checked.so): every index the step kernels take
+// from their tables is range-checked on the device before it is used, and a violation sets
+// bit 2 of the error word (the host reports HCFD_EINVAL).  The tiled kernels check their
+// plan's indices (tile descriptors, halo ids, cell slots, entry metadata) where they read
+// them, replacing a bad one by an index in range or skipping the access; the per-cell
+// kernels' slot table is checked by check_slots_kernel before a step, and no step is launched
+// on a bad one.  The default build relies on the host-side checks of every mesh and plan
+// (validate_view, the plan builder, hcfd_plan_check) and compiles without the checks.
+#ifdef HCFD_CHECKED
+constexpr bool kChecked = true;
+#else
+constexpr bool kChecked = false;
+#endif
+__device__ __forceinline__ bool index_ok(bool ok, unsigned int* err) {
+    if (kChecked && !ok) atomicOr(err, 4u);
+    return !kChecked || ok;
+}
 template <class T>
 struct StepArgs {
     const Cell4<T>* __restrict__ U;      // state at step start
@@ -320,6 +337,20 @@ __device__ __forceinline__ double warp_sum(double x) {
 
 // ---------------------------------------------------------------------------------------
 // pass 1: gradient + limiter (+ CFL minimum)
+
+// Checked build: every face and neighbour id of the per-cell kernels' slot table ([W][Nc]
+// int2: {face or ~face, neighbour}, neighbour -1 for an unused slot) checked on the device
+// before a step; a bad one sets bit 2 of err and the host launches no step.  The per-cell step
+// kernels themselves carry no checks, so they are the default build's code.
+static __global__ void check_slots_kernel(const int2* __restrict__ slot, int W, int Nc, int Nf, unsigned int* err) {
+    const size_t n = (size_t) W * Nc;
+    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x) {
+        const int2 s = slot[i];
+        if (s.y < 0) continue;
+        const int f = s.x >= 0 ? s.x : ~s.x;
+        if (f >= Nf || s.y >= Nc) atomicOr(err, 4u);
+    }
+}
 
 template <class T, int W>
 __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {

@@ -16,6 +16,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -32,6 +33,7 @@ constexpr size_t kPhiG = 0;                                                   //
 constexpr size_t kPartial = kPhiG + (size_t) 64 * HCFD_NOALLOC_MAX_CELLS;     // double[kMaxBlocks]
 constexpr size_t kDtmin = kPartial + ((sizeof(double) * kMaxBlocks + 255) & ~(size_t) 255);  // u64[2]
 constexpr size_t kCounter = kDtmin + 256;                                     // unsigned int
+constexpr size_t kErr = kCounter + 128;                                       // unsigned int (checked build)
 constexpr size_t kStats = kCounter + 256;                                     // StepStats
 constexpr size_t kScratchBytes = kStats + 256;
 
@@ -78,11 +80,13 @@ unsigned long long current_ctx_id() {
 }
 
 // Clears what must start at zero (and the dt minimum at +inf) on every call.
-__global__ void noalloc_reset_kernel(unsigned long long* dtmin, unsigned int* counter, hcfd::StepStats* stats) {
+__global__ void noalloc_reset_kernel(unsigned long long* dtmin, unsigned int* counter, unsigned int* err,
+                                     hcfd::StepStats* stats) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         dtmin[0] = 0x7FF0000000000000ULL;
         dtmin[1] = 0x7FF0000000000000ULL;
         *counter = 0u;
+        *err = 0u;
         hcfd::StepStats z{};
         *stats = z;
     }
@@ -186,7 +190,21 @@ extern "C" int hcfd_step_noalloc(const hcfd_noalloc_mesh* m, const double* U_in,
     a.freeze_after = 0;
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    noalloc_reset_kernel<<<1, 32, 0, st>>>(a.dtmin, a.counter, a.stats);
+    unsigned int* d_err = reinterpret_cast<unsigned int*>(base + kErr);
+    noalloc_reset_kernel<<<1, 32, 0, st>>>(a.dtmin, a.counter, d_err, a.stats);
+    if constexpr (hcfd::kChecked) {
+        // checked build: the caller's slot table is checked on the device before the step,
+        // which is not launched when an id is out of range
+        const long long n = (long long) m->slots * m->Nc;
+        hcfd::check_slots_kernel<<<(int) std::min<long long>((n + 255) / 256, 1184), 256, 0, st>>>(
+            a.slot, m->slots, m->Nc, m->Nf, d_err);
+        unsigned int err = 0;
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&err, d_err, sizeof(err), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(HCFD_ECUDA, std::string("step_noalloc: ") + cudaGetErrorString(e));
+        if (err & 4u) return fail(HCFD_EINVAL, "step_noalloc, checked build: a face or neighbour id was out of range");
+    }
     switch (m->slots) {
     case 3: launch<3>(a, st); break;
     case 4: launch<4>(a, st); break;

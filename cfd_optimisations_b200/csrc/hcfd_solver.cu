@@ -193,6 +193,9 @@ hcfd::TileArgs<T> tile_args(hcfd_solver* s, int time_mode, double dt_or_cfl, con
     a.Wp = P.plan.Wp;
     a.Hmax = P.plan.Hmax;
     a.Fmax = P.plan.Fmax;
+    a.nentries = (long long) P.plan.efid.size();
+    a.nhalo = (long long) P.plan.halo.size();
+    a.ncap = (long long) P.plan.ntiles * P.plan.B;
     a.err = s->d_err;
     a.polls = s->wait_polls;
     a.skip_tile = s->wait_skip_tile;
@@ -329,6 +332,7 @@ int read_stats(hcfd_solver* s, hcfd_step_stats* out) {
         out->steps = st.steps;
         out->nonfinite = st.nonfinite;
     }
+    if (err & 4u) return fail(HCFD_EINVAL, "checked build: a tile index was out of range (corrupt tile plan)");
     if (err) return fail(HCFD_ETIMEOUT, "a bounded device wait gave up (tile staging did not complete)");
     return st.nonfinite ? fail(HCFD_ENONFINITE, "a step produced a NaN or Inf") : HCFD_OK;
 }
@@ -633,6 +637,20 @@ int hcfd_gpu_step(hcfd_solver* s, int nsteps, int time_mode, double dt_or_cfl, h
     if (!s->initialised) return fail(HCFD_EINVAL, "step: call initialise first");
     if (nsteps < 0 || time_mode < HCFD_FIXED_DT || time_mode > HCFD_LOCAL_CFL || !std::isfinite(dt_or_cfl) || dt_or_cfl < 0)
         return fail(HCFD_EINVAL, "step: bad argument");
+    if constexpr (hcfd::kChecked) {
+        // checked build: the per-cell kernels' slot table is checked on the device before
+        // any step (the tiled kernels check their plan's indices as they read them)
+        if (!s->tiled && nsteps > 0) {
+            const long long n = (long long) s->W * s->Nc;
+            hcfd::check_slots_kernel<<<(int) std::min<long long>((n + 255) / 256, 1184), 256, 0, s->stream>>>(
+                s->d_slot, s->W, s->Nc, s->Nf, s->d_err);
+            CK(cudaGetLastError());
+            unsigned int err = 0;
+            CK(cudaMemcpyAsync(&err, s->d_err, sizeof(err), cudaMemcpyDeviceToHost, s->stream));
+            CK(cudaStreamSynchronize(s->stream));
+            if (err & 4u) return fail(HCFD_EINVAL, "checked build: a face or neighbour id of the slot table is out of range");
+        }
+    }
     int n = nsteps;
     while (n > 0) {
         // pairs of steps without per-kernel events run as the graph; profiled steps run eagerly

@@ -30,7 +30,8 @@ struct TileArgs {
     const int* __restrict__ halo;          // internal cell ids
     const short* __restrict__ cslot;       // [ntiles * B * Wp]: (entry << 1) | cell-is-right, or -1; Wp = W
     int ntiles, B, Wp, Hmax, Fmax;
-    unsigned int* err;                     // bit 0: a bounded wait gave up; bit 1: copies did not drain
+    unsigned int* err;                     // bit 0: a bounded wait gave up; bit 1: copies did not drain;
+                                           // bit 2: an index out of range (checked build)
     unsigned polls;                        // poll limit of every bounded wait (2^22 by default)
     int skip_tile;                         // failure injection for tests: the producer arms nothing
                                            // for this tile (-1: none)
@@ -46,6 +47,8 @@ struct TileArgs {
     double* tile_r2;                       // per active tile and compute warp (t * B/32 + warp): sum of R_rho^2
     int* tile_bad;                         // same layout: a NaN/Inf appeared
     int par;                               // which dtmin slot this step uses
+    long long nentries, nhalo, ncap;       // lengths of tgeo/tmeta (entries), halo, and of the
+                                           // per-cell arrays iv/cslot (cells): checked build
 };
 
 // Metadata of a face entry in one 32-bit word: the local index (tile cell 0..B-1, halo cell
@@ -63,6 +66,15 @@ inline std::vector<unsigned> packed_meta(const TilePlan& P) {
 __device__ __forceinline__ int meta_la(unsigned w) { return (int) (w & 0x1FFFu); }
 __device__ __forceinline__ int meta_lb(unsigned w) { return (int) ((w >> 13) & 0x1FFFu); }
 __device__ __forceinline__ int meta_bc(unsigned w) { return (int) (w >> 26) - 1; }
+
+// A local cell index of a tile: one of its nb cells, or one of its nh halo cells (B..).
+__device__ __forceinline__ bool local_ok(int l, int nb, int B, int nh) {
+    return (l >= 0 && l < nb) || (l >= B && l < B + nh);
+}
+// A face entry's metadata: both cells local to the tile, the boundary condition in the table.
+__device__ __forceinline__ bool entry_ok(unsigned w, int nb, int B, int nh, unsigned int* err) {
+    return index_ok(local_ok(meta_la(w), nb, B, nh) && local_ok(meta_lb(w), nb, B, nh) && meta_bc(w) < MAXBC, err);
+}
 
 // Cells, face entries and halo of tile t (single mesh) or of active tile t (arena).
 template <bool ARENA, class T>
@@ -311,6 +323,14 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
         if (iter >= 2 && !__all_sync(0xffffffffu, mbar_wait(empty + buf, ((iter >> 1) - 1) & 1, a.polls, a.err, abort)))
             break;
         if (t == a.skip_tile) continue;      // failure injection: nothing armed, nothing in flight
+        bool good = true;
+        if constexpr (kChecked) {
+            // a descriptor outside the arrays or the staging capacity: the tile is staged empty
+            good = index_ok(base >= 0 && nb >= 0 && nb <= a.B && base + nb <= a.ps && base + a.B <= a.ncap &&
+                            f0 >= 0 && nf >= 0 && nf <= a.Fmax && f0 + nf <= a.nentries &&
+                            h0 >= 0 && nh >= 0 && nh <= a.Hmax && h0 + nh <= a.nhalo, a.err);
+            if (!good) nb = nf = nh = 0;
+        }
         unsigned char* st = smem + kHeader + buf * L.stage;
         Cell4<T>* sU = reinterpret_cast<Cell4<T>*>(st + L.u);
         Grad8<T>* sG = reinterpret_cast<Grad8<T>*>(st + L.g);
@@ -326,6 +346,9 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
             si->dt_or_cfl = v_dt;
             si->dtmin = v_dtmin;
             si->steps = v_steps;
+            if (!good) {
+                mbar_arrive_expect_tx(full + buf, 0u);   // nothing copied (checked build)
+            } else {
             mbar_arrive_expect_tx(full + buf, bu + bg + bf + bm + bs + bi);
             // one bulk copy per 16-byte chunk plane of the tile's cell range
 #pragma unroll
@@ -345,9 +368,11 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
             }
             bulk_g2s(st + L.cslot, a.cslot + (size_t) base * a.Wp, bs, full + buf);
             bulk_g2s(st + L.iv, a.s.iv + base, bi, full + buf);
+            }
         }
         for (int h = lane; h < nh; h += 32) {
             const int ci = __ldg(a.halo + h0 + h);
+            if (!index_ok(ci >= 0 && ci < a.ps, a.err)) continue;
 #pragma unroll
             for (int j = 0; j < CU; j++)
                 cp_async16(reinterpret_cast<char*>(sU) + 16 * ((size_t) j * NL + a.B + h),
@@ -565,11 +590,15 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
         for (int k = 0; k < W; k++) {
             ro[k][0] = T(0); ro[k][1] = T(0);
             if (cs[k] < 0) continue;
-            const int e = cs[k] >> 1;
+            int e = cs[k] >> 1;
             const bool isL = (cs[k] & 1) == 0;
+            if constexpr (kChecked)    // a bad index is replaced by entry 0 / tile cell 0 (no branch)
+                e = index_ok(e < nfl, a.err) ? e : 0;
             FaceGeo<T> g;
             lds_geo4(sGeo, nfl, e, g);
-            const int nbl = isL ? meta_lb(sMeta[e]) : meta_la(sMeta[e]);
+            int nbl = isL ? meta_lb(sMeta[e]) : meta_la(sMeta[e]);
+            if constexpr (kChecked)
+                nbl = index_ok(local_ok(nbl, nb, a.B, si.nh), a.err) ? nbl : 0;
             T un[4];
             lds_cell(sU, NL, nbl, un);
             // GaussGreen.cpp:25-28: uf = u_CL If + u_CR (1 - If), added into CL and taken from
@@ -683,6 +712,8 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
         const int pairs = min(NT, max(0, nf - base2 - NT));      // threads with a second entry
         if (sizeof(T) == 4 || (int) (threadIdx.x & ~31u) < pairs) {
             const int eB = (e + NT < nf) ? e + NT : e;
+            if constexpr (kChecked)
+                if (!entry_ok(sMeta[e], nb, a.B, si.nh, a.err) || !entry_ok(sMeta[eB], nb, a.B, si.nh, a.err)) continue;
             FaceIn<T> A, Bq;
             A.load(sU, sG, NL, sGeo, sMeta, nf, a.rec, e);
             Bq.load(sU, sG, NL, sGeo, sMeta, nf, a.rec, eB);
@@ -692,6 +723,8 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
             A.template store<COMP>(sGeoW, nf, a.rec, FA);
             if (eB != e) Bq.template store<COMP>(sGeoW, nf, a.rec, FB);
         } else {
+            if constexpr (kChecked)
+                if (!entry_ok(sMeta[e], nb, a.B, si.nh, a.err)) continue;
             FaceIn<T> A;
             A.load(sU, sG, NL, sGeo, sMeta, nf, a.rec, e);
             T FA[4];
@@ -718,7 +751,9 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
         for (int k = 0; k < W; k++) {
             if (cs[k] < 0) continue;
             const bool isL = (cs[k] & 1) == 0;
-            const int e = cs[k] >> 1;
+            int e = cs[k] >> 1;
+            if constexpr (kChecked)
+                e = index_ok(e < nf, a.err) ? e : 0;
             const int rp = rplane(a.rec);
             const auto F01 = ldp(sGeo, nf, rp, e), F23 = ldp(sGeo, nf, rp + 1, e);
             const T Fk[4] = {F01.x, F01.y, F23.x, F23.y};
@@ -762,7 +797,9 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
             const int bc = meta_bc(w);
             if (bc < 0) continue;
             const int lb = meta_lb(w);
+            if (!index_ok(local_ok(lb, nb, a.B, si.nh) && bc < MAXBC, a.err)) continue;
             const int gi = lb < a.B ? base + lb : __ldg(a.halo + h0t + lb - a.B);
+            if (!index_ok(gi >= 0 && gi < a.ps, a.err)) continue;
             T gnx, gny, gA;
             lds_geo3(sGeo, nf, e, a.rec, gnx, gny, gA);
             T ug[4];

@@ -1,6 +1,8 @@
 """ctypes binding of libhcfd_gpu.so (include/hcfd_gpu.h).
 
-Loading fails loudly when the library is missing: there is no CPU fallback.
+Loading fails loudly when the library is missing: there is no CPU fallback.  HCFD_LIB=checked
+selects the checked twin libhcfd_gpu_checked.so (same entry points; its tile kernels verify
+every index they read and report a bad one as HCFD_EINVAL instead of reading out of bounds).
 """
 from __future__ import annotations
 
@@ -8,7 +10,12 @@ import ctypes as ct
 import os
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "lib", "libhcfd_gpu.so")
+LIB_DEFAULT = os.path.join(PKG, "lib", "libhcfd_gpu.so")
+LIB_CHECKED = os.path.join(PKG, "lib", "libhcfd_gpu_checked.so")
+_choice = os.environ.get("HCFD_LIB", "")
+if _choice not in ("", "default", "checked"):
+    raise RuntimeError(f"HCFD_LIB={_choice!r}: expected 'default' or 'checked'")
+LIB_PATH = LIB_CHECKED if _choice == "checked" else LIB_DEFAULT
 
 # status codes (include/hcfd_gpu.h)
 OK, EINVAL, ENOMEM, ECUDA, ENONFINITE, ETIMEOUT, EIO, EAGAIN = 0, -1, -2, -3, -4, -5, -6, -7

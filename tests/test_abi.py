@@ -24,10 +24,11 @@ def declared():
     return names
 
 
-def test_every_declared_symbol_is_exported():
+@pytest.mark.parametrize("path", [N.LIB_DEFAULT, N.LIB_CHECKED], ids=["default", "checked"])
+def test_every_declared_symbol_is_exported(path):
     names = declared()
     assert len(names) >= 30
-    out = subprocess.run(["nm", "-D", "--defined-only", N.LIB_PATH], capture_output=True, text=True).stdout
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
     exported = set(re.findall(r"\bT (hcfd_[a-z0-9_]+)\b", out))
     assert names <= exported, sorted(names - exported)
 
