@@ -97,6 +97,9 @@ struct hcfd_solver {
     bool split = false;                  // pass 2 uses tp[1]
     size_t smem1 = 0, smem2 = 0;
     int grid1 = 0, grid2 = 0;
+    // tile queues (d_counter[1] for pass 1, d_counter[2] for pass 2): CTAs that finish
+    // early take more tiles; without, every CTA takes every grid-th tile
+    bool queue1 = true, queue2 = false;
     bool tiled = false;
     int cur = 0;                         // which of d_U holds the state
     int block = 256;
@@ -178,8 +181,12 @@ hcfd::StepArgs<T> step_args(hcfd_solver* s, int time_mode, double dt_or_cfl) {
 }
 
 template <class T>
-hcfd::TileArgs<T> tile_args(hcfd_solver* s, int time_mode, double dt_or_cfl, const TiledPass& P) {
+hcfd::TileArgs<T> tile_args(hcfd_solver* s, int time_mode, double dt_or_cfl, const TiledPass& P, int pass) {
     hcfd::TileArgs<T> a;
+    int* q1 = s->queue1 ? (int*) s->d_counter + 1 : nullptr;
+    int* q2 = s->queue2 ? (int*) s->d_counter + 2 : nullptr;
+    a.claim = pass == 1 ? q1 : q2;
+    a.claim_reset = pass == 1 ? q2 : q1;
     a.s = step_args<T>(s, time_mode, dt_or_cfl);
     a.tgeo = (const T*) P.d_tgeo;
     a.rec = P.rec;
@@ -236,8 +243,8 @@ int launch_step(hcfd_solver* s, int time_mode, double dt_or_cfl) {
     const bool rec = s->prof && (s->prof_count++ % s->prof_every == 0);
     if (s->tiled) {
         const TiledPass& P2 = s->split ? s->tp[1] : s->tp[0];
-        const hcfd::TileArgs<T> a1 = tile_args<T>(s, time_mode, dt_or_cfl, s->tp[0]);
-        const hcfd::TileArgs<T> a2 = tile_args<T>(s, time_mode, dt_or_cfl, P2);
+        const hcfd::TileArgs<T> a1 = tile_args<T>(s, time_mode, dt_or_cfl, s->tp[0], 1);
+        const hcfd::TileArgs<T> a2 = tile_args<T>(s, time_mode, dt_or_cfl, P2, 2);
         if ((rc = prof_begin(s, rec, e1))) return rc;
         hcfd::tile_pass1_kernel<T, W, false><<<s->grid1, s->tp[0].block + 32, s->smem1, s->stream>>>(a1);
         if ((rc = prof_end(s, rec, e1, s->ev1))) return rc;
@@ -486,7 +493,7 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         (rc = dalloc((char**) &h->d_phiG, tsz * 8 * Nc)) || (rc = dalloc(&h->d_io, 4 * (size_t) Nc)) ||
         (p.freeze_limiter_after > 0 && (rc = dalloc((char**) &h->d_phiF, tsz * 4 * Nc))) ||
         (rc = dalloc(&h->d_cp, Nf)) || (rc = dalloc(&h->d_dtmin, 2)) || (rc = dalloc(&h->d_partial, h->partial_len)) ||
-        (rc = dalloc(&h->d_counter, 1)) || (rc = dalloc(&h->d_err, 1)) || (rc = dalloc(&h->d_stats, 1)) ||
+        (rc = dalloc(&h->d_counter, 4)) || (rc = dalloc(&h->d_err, 1)) || (rc = dalloc(&h->d_stats, 1)) ||
         (rc = dalloc(&d_fn, 2 * (size_t) Nf)) || (rc = dalloc(&d_fcu, 2 * (size_t) Nf)) ||
         (rc = dalloc(&d_cnoff, Nc + 1)) || (rc = dalloc(&d_cncon, ncn)) || (rc = dalloc(&d_cfoff, Nc + 1)) ||
         (rc = dalloc(&d_cfcon, cf_con.size())) || (rc = dalloc(&d_nodes, 2 * (size_t) h->Nn)) ||
@@ -567,7 +574,7 @@ int hcfd_gpu_create(const hcfd_mesh_view* mv, const hcfd_params* prm, hcfd_solve
         const unsigned long long inf2[2] = {0x7FF0000000000000ULL, 0x7FF0000000000000ULL};
         ce = up(h->d_dtmin, inf2, sizeof(inf2));
     }
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned int), st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_counter, 0, 4 * sizeof(unsigned int), st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_err, 0, sizeof(unsigned int), st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_stats, 0, sizeof(hcfd::StepStats), st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_phiG, 0, tsz * 8 * Nc, st);
@@ -623,6 +630,7 @@ int hcfd_gpu_initialise(hcfd_solver* s, const double* qic) {
     if (rc) return rc;
     CK(cudaMemsetAsync(s->d_stats, 0, sizeof(hcfd::StepStats), s->stream));
     CK(cudaMemsetAsync(s->d_err, 0, sizeof(unsigned int), s->stream));
+    CK(cudaMemsetAsync(s->d_counter, 0, 4 * sizeof(unsigned int), s->stream));   // ticket, tile queues
     const unsigned long long inf2[2] = {0x7FF0000000000000ULL, 0x7FF0000000000000ULL};
     CK(cudaMemcpyAsync(s->d_dtmin, inf2, sizeof(inf2), cudaMemcpyHostToDevice, s->stream));
     CK(cudaStreamSynchronize(s->stream));

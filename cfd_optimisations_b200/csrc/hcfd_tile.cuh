@@ -47,6 +47,12 @@ struct TileArgs {
     double* tile_r2;                       // per active tile and compute warp (t * B/32 + warp): sum of R_rho^2
     int* tile_bad;                         // same layout: a NaN/Inf appeared
     int par;                               // which dtmin slot this step uses
+    // Tile queue: each CTA takes tile blockIdx.x first, then, with `claim` set, the tile
+    // gridDim.x + atomicAdd(claim, 1) (CTAs that finish early take more tiles), else every
+    // gridDim.x-th tile.  `claim_reset` (the other pass's queue) is zeroed by this kernel:
+    // the other pass runs before and after it in stream order, never during it.
+    int* claim;
+    int* claim_reset;
     long long nentries, nhalo, ncap;       // lengths of tgeo/tmeta (entries), halo, and of the
                                            // per-cell arrays iv/cslot (cells): checked build
 };
@@ -100,7 +106,8 @@ struct StageInfo {
     double dt_or_cfl;
     double dtmin;
     long long steps;
-    long long pad2;
+    int t;                                            // the tile, or -1: the CTA has no more tiles
+    int pad2;
 };
 static_assert(sizeof(StageInfo) == 64, "stage info is 64 bytes");
 // Header of a CTA's shared memory: full[2] and empty[2] mbarriers (bytes 0-31), the abort
@@ -287,6 +294,15 @@ __device__ __forceinline__ void compute_sync(int nthreads) {
 // Once any wait of the CTA has given up, the producer issues nothing more; before it
 // returns it waits for the copies it has issued (the last armed phase of each buffer; earlier
 // ones completed before their buffer was re-armed), so no copy lands after the CTA exits.
+// The CTA's tile after tile t (all 32 lanes of the producer warp call it together).
+template <class T>
+__device__ __forceinline__ int next_tile(const TileArgs<T>& a, int t, int lane) {
+    if (!a.claim) return t + (int) gridDim.x;
+    int n = 0;
+    if (lane == 0) n = (int) gridDim.x + atomicAdd(a.claim, 1);
+    return __shfl_sync(0xffffffffu, n, 0);
+}
+
 template <class T, bool PASS2, bool ARENA>
 __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned char* smem, unsigned long long* full,
                                               unsigned long long* empty, const TileSmem<T>& L) {
@@ -296,9 +312,25 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
     volatile int* abort = abort_word(smem);
     int armed[2] = {-1, -1};       // last iteration whose copies were issued into each buffer
     unsigned iter = 0;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {
+    // the tile after the current one is taken one iteration ahead, so that the latency of a
+    // claim hides behind the current tile
+    int t = blockIdx.x;
+    int tn = next_tile(a, t, lane);
+    for (;; iter++, t = tn, tn = t < a.ntiles ? next_tile(a, t, lane) : t) {
         const int buf = iter & 1;
         if (__any_sync(0xffffffffu, *abort)) break;
+        if (t >= a.ntiles) {
+            // no more tiles: a stage with tile -1 and nothing copied ends the compute warps' loop
+            if (iter >= 2 && !__all_sync(0xffffffffu, mbar_wait(empty + buf, ((iter >> 1) - 1) & 1, a.polls, a.err, abort)))
+                break;
+            if (lane == 0) {
+                reinterpret_cast<StageInfo*>(smem + 64)[buf].t = -1;
+                mbar_arrive_expect_tx(full + buf, 0u);
+            }
+            cp_async_arrive_noinc(full + buf);
+            armed[buf] = (int) iter;
+            break;
+        }
         // the tile's descriptor and its instance's scalars are loaded before the wait for the
         // stage, so that their latency hides behind it (none of them changes during the kernel
         // in a way the kernel reads: dt minima and step counts come from earlier kernels)
@@ -312,7 +344,6 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
                 v_dt = __ldg(a.inst_dt + inst);
                 v_dtmin = __longlong_as_double((long long) a.inst_dtmin[2 * inst + a.par]);
                 v_steps = a.inst_stats[inst].steps;
-                const int tn = t + (int) gridDim.x;
                 if (!PASS2 && tn < a.ntiles) v_next = __ldg(&a.tiles[2 * tn].w);
             } else {
                 v_dt = a.s.dt_or_cfl;
@@ -342,6 +373,7 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
             // arrive below
             StageInfo* si = reinterpret_cast<StageInfo*>(smem + 64) + buf;
             si->base = base; si->nb = nb; si->f0 = f0; si->nf = nf; si->h0 = h0; si->nh = nh; si->inst = inst;
+            si->t = t;
             si->next_inst = v_next;                  // pass 1 in arena mode only
             si->dt_or_cfl = v_dt;
             si->dtmin = v_dtmin;
@@ -520,7 +552,10 @@ struct FaceIn {
 // Warp-specialised persistent tile loop.  The last warp of the CTA is the producer
 // (producer_loop); the first NT = blockDim.x - 32 threads compute.  Compute iteration i
 // reads staging buffer i & 1 once its `full` barrier completes and releases it on its
-// `empty` barrier (one arrival per compute warp) when done.
+// `empty` barrier (one arrival per compute warp) when done.  The tile comes with the stage
+// (StageInfo::t); after the CTA's last tile the producer stages tile -1 with nothing copied,
+// and the compute warps leave the loop on it (in pass 2 after the face-phase barrier, which
+// every compute warp meets once more).
 // A compute warp whose stage wait gives up reads nothing of that stage.  In pass 1 (no
 // barrier among the compute warps inside the loop) it leaves the loop at once.  In pass 2
 // it marks the compute abort word and skips the face phase (`staged` false); every compute
@@ -542,8 +577,8 @@ struct FaceIn {
     if ((int) threadIdx.x >= NT) {                                                               \
         producer_loop<T, PASS2, ARENA>(a, smem, full, empty, L);                                 \
     } else {                                                                                     \
-    unsigned iter = 0;                                                                           \
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, iter++) {                             \
+    if (a.claim_reset && blockIdx.x == 0 && threadIdx.x == 0) *a.claim_reset = 0;               \
+    for (unsigned iter = 0;; iter++) {                                                           \
         const int buf = iter & 1;                                                                \
         unsigned char* st = smem + kHeader + buf * L.stage;                                      \
         const bool staged = __all_sync(0xffffffffu,                                              \
@@ -552,6 +587,9 @@ struct FaceIn {
         if (!PASS2 && !staged) break;                                                            \
         if (PASS2 && !staged && (threadIdx.x & 31) == 0) *compute_abort_word(smem) = 1;          \
         const StageInfo& si = reinterpret_cast<const StageInfo*>(smem + 64)[buf];                \
+        const int t = staged ? si.t : 0;                                                         \
+        const bool fin = staged && t < 0;     /* the producer has no more tiles */               \
+        if (!PASS2 && fin) break;                                                                \
         const int base = si.base, nb = si.nb, h0t = si.h0, inst = si.inst;                      \
         const Cell4<T>* sU = reinterpret_cast<const Cell4<T>*>(st + L.u);                        \
         const T* sGeo = reinterpret_cast<const T*>(st + L.geo);                                  \
@@ -694,9 +732,10 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
     int bad = 0;
     HCFD_TILE_LOOP_BEGIN(true, ARENA)
     const T cfl_or_dt = T(si.dt_or_cfl);
-    dt_used = (s.time_mode == TM_FIXED) ? si.dt_or_cfl : si.dt_or_cfl * si.dtmin;
+    if (staged && !fin) dt_used = (s.time_mode == TM_FIXED) ? si.dt_or_cfl : si.dt_or_cfl * si.dtmin;
     const Grad8<T>* sG = reinterpret_cast<const Grad8<T>*>(st + L.g);
-    const int nf = staged ? nfl : 0;         // a stage whose wait gave up is not read
+    // a stage whose wait gave up is not read, nor the closing stage (tile -1)
+    const int nf = (staged && !fin) ? nfl : 0;
     // face phase: one Rusanov flux per face entry (Flux.cpp:19-38).  Each thread takes two
     // entries per round and computes both before storing either, so the two independent
     // FP64 dependency chains (divisions, square roots) interleave.
@@ -733,7 +772,9 @@ __global__ void __maxnreg__(128) tile_pass2_kernel(const TileArgs<T> a) {
         }
     }
     compute_sync(NT);
-    if (*compute_abort_word(smem)) break;    // some compute warp's stage wait gave up
+    // some compute warp's stage wait gave up, or the closing stage (every compute warp that
+    // read the stage sees its tile -1; one whose wait gave up sees the abort word)
+    if (*compute_abort_word(smem) || fin) break;
     // cell phase: slots in increasing face order, update, ghost refresh
     for (int c = threadIdx.x; c < nb; c += NT) {
         short cs[8];
