@@ -294,13 +294,17 @@ __device__ __forceinline__ void compute_sync(int nthreads) {
 // Once any wait of the CTA has given up, the producer issues nothing more; before it
 // returns it waits for the copies it has issued (the last armed phase of each buffer; earlier
 // ones completed before their buffer was re-armed), so no copy lands after the CTA exits.
-// The CTA's tile after tile t (all 32 lanes of the producer warp call it together).
+// Tile queue: lane 0 of the producer warp issues the claim of a tile at the top of an
+// iteration (claim_issue) and the warp takes its result at the end (claim_take), so that the
+// atomic's round trip overlaps the iteration's staging.
 template <class T>
-__device__ __forceinline__ int next_tile(const TileArgs<T>& a, int t, int lane) {
+__device__ __forceinline__ int claim_issue(const TileArgs<T>& a, int lane) {
+    return (a.claim && lane == 0) ? atomicAdd(a.claim, 1) : 0;
+}
+template <class T>
+__device__ __forceinline__ int claim_take(const TileArgs<T>& a, int t, int pending) {
     if (!a.claim) return t + (int) gridDim.x;
-    int n = 0;
-    if (lane == 0) n = (int) gridDim.x + atomicAdd(a.claim, 1);
-    return __shfl_sync(0xffffffffu, n, 0);
+    return (int) gridDim.x + __shfl_sync(0xffffffffu, pending, 0);
 }
 
 template <class T, bool PASS2, bool ARENA>
@@ -312,12 +316,14 @@ __device__ __forceinline__ void producer_loop(const TileArgs<T>& a, unsigned cha
     volatile int* abort = abort_word(smem);
     int armed[2] = {-1, -1};       // last iteration whose copies were issued into each buffer
     unsigned iter = 0;
-    // the tile after the current one is taken one iteration ahead, so that the latency of a
-    // claim hides behind the current tile
+    // the current tile t and the next tn are known at the top of an iteration; the tile after
+    // tn is claimed during the iteration
     int t = blockIdx.x;
-    int tn = next_tile(a, t, lane);
-    for (;; iter++, t = tn, tn = t < a.ntiles ? next_tile(a, t, lane) : t) {
+    int tn = claim_take(a, t, claim_issue(a, lane));
+    int pending = 0;
+    for (;; iter++, t = tn, tn = t < a.ntiles ? claim_take(a, t, pending) : t) {
         const int buf = iter & 1;
+        if (tn < a.ntiles) pending = claim_issue(a, lane);
         if (__any_sync(0xffffffffu, *abort)) break;
         if (t >= a.ntiles) {
             // no more tiles: a stage with tile -1 and nothing copied ends the compute warps' loop
