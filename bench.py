@@ -57,9 +57,9 @@ VENKAT_K, CFL = 5.0, 0.5
 REF_MAX_STEPS, REF_MAX_WARMUP = 60, 5      # keeps the reference arm within about two minutes
 
 
-def workload() -> str:
+def workload(precision: str = "fp64") -> str:
     return (f"supersonic wedge {NX}x{NY} nodes ({2 * (NX - 1) * (NY - 1):,} triangles), M{MACH} "
-            f"{THETA:g}deg, Venkatakrishnan K{VENKAT_K:g}, global CFL {CFL}, FP64, RCM numbering")
+            f"{THETA:g}deg, Venkatakrishnan K{VENKAT_K:g}, global CFL {CFL}, {precision.upper()}, RCM numbering")
 
 
 def freestream_case(mach: float = MACH, rho: float = 1.4, p: float = 1.0, gma: float = 1.4):
@@ -309,6 +309,8 @@ def main():
     ap.add_argument("--mesh", default=f"{NX}x{NY}", help="node grid NXxNY (profiling of smaller cases)")
     ap.add_argument("--kernel", choices=["tiled", "cell"], default="tiled",
                     help="step kernel family (the per-cell gather kernels are the other fusion split)")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
+                    help="precision of the headline solve (FP64 is the headline; FP32 for profiling its kernels)")
     ap.add_argument("--profile-only", action="store_true",
                     help="warm-up and timed steps only (no end-to-end, variants, CPU, batched or served legs): for ncu")
     ap.add_argument("--tour", action="store_true",
@@ -331,7 +333,9 @@ def main():
     mesh = make_mesh(H.NUMBER_RCM)
     bcmap, qbc, q = H.wedge_case(MACH)
     kernel = H.KERNEL_CELL if args.kernel == "cell" else H.KERNEL_TILED
-    s = H.Solver(mesh, limiter=H.LIMITER_VENKAT, venkat_K=VENKAT_K, precision=H.FP64, kernel=kernel)
+    f32 = args.precision == "fp32"
+    s = H.Solver(mesh, limiter=H.LIMITER_VENKAT, venkat_K=VENKAT_K, precision=H.FP32 if f32 else H.FP64,
+                 kernel=kernel)
     s.gather_bcs(bcmap, qbc)
     s.initialise(q)
     ntri = s.Nreal
@@ -352,10 +356,11 @@ def main():
     ms_max = allmax(dist, ms)
     value = aggregate(ntri * args.steps, world, ms_max)
 
-    # Roofline of the dominant kernel.  Algorithmic bytes (two-pass minimum, w = 8):
+    # Roofline of the dominant kernel.  Algorithmic bytes (two-pass minimum, w = 8 in FP64,
+    # 4 in FP32):
     #   pass 1: U (4w) + iv (w) + phiG (8w) per cell, (8 + 7w) per face
     #   pass 2: U (4w) + phiG (8w) + iv (w) + U' (4w) per cell, (8 + 7w) per face
-    w = 8
+    w = 4 if f32 else 8
     b1 = 13 * w * Nc + (8 + 7 * w) * Nf
     b2 = 17 * w * Nc + (8 + 7 * w) * Nf
     t1 = prof["ms_pass1"] / max(prof["n_pass1"], 1)
@@ -364,13 +369,13 @@ def main():
     peak, peak_kind = peaks()
     achieved = b / (t * 1e-3) / 1e9
     step_achieved = (b1 + b2) / (ms_max / args.steps * 1e-3) / 1e9
-    traffic = traffic_from_profiles(dom, f"fp64_rcm_{NX}x{NY}" + ("_cell" if args.kernel == "cell" else ""))
+    traffic = traffic_from_profiles(dom, f"{args.precision}_rcm_{NX}x{NY}" + ("_cell" if args.kernel == "cell" else ""))
 
     line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if f32 else "f64",
             "data": "synthetic",
-            "config": {"workload": workload() + (", per-cell kernels" if args.kernel == "cell" else ""),
+            "config": {"workload": workload(args.precision) + (", per-cell kernels" if args.kernel == "cell" else ""),
                        "cells": Nc, "real_cells": ntri, "faces": Nf,
                        "parallelism": f"{world} replica(s), one per GPU, no collective",
                        "l2": "per-step working set > 1.6 GB, far above the 126 MB L2; no flush"},
