@@ -241,6 +241,7 @@ struct hcfd_arena {
     double* tile_r2 = nullptr;
     int* tile_bad = nullptr;
     unsigned int* err = nullptr;
+    int* queue = nullptr;                // pass 1's tile queue (see TileArgs::claim)
     size_t tiles_cap = 0;
     // host
     std::vector<Inst> inst;
@@ -330,7 +331,14 @@ template <class T, int W>
 int enqueue_step(hcfd_arena* A, int cur, int par) {
     hcfd::TileArgs<T> a = arena_args<T>(A, cur, par);
     constexpr bool COMP = std::is_same<T, float>::value;
+    // pass 1 takes its tiles from a queue (per-instance dt minima are order-free), and pass 2,
+    // which runs between two pass-1 launches, zeroes it; pass 2 takes every grid-th tile
+    // (measured faster for it than a queue)
+    a.claim = A->queue;
+    a.claim_reset = nullptr;
     hcfd::tile_pass1_kernel<T, W, true><<<A->grid1, A->B + 32, A->smem1, A->stream>>>(a);
+    a.claim = nullptr;
+    a.claim_reset = A->queue;
     hcfd::tile_pass2_kernel<T, W, COMP, true><<<A->grid2, A->B + 32, A->smem2, A->stream>>>(a);
     arena_chunk_kernel<<<A->nchunks, 256, 0, A->stream>>>(A->chunks, A->tile_r2, A->tile_bad, A->chunk_r2, A->chunk_bad);
     arena_finalize_kernel<<<(A->nact + 127) / 128, 128, 0, A->stream>>>(A->nact, A->nchunks, A->act, A->chunk_r2,
@@ -447,8 +455,8 @@ void arena_free(hcfd_arena* A) {
     if (A->list_ev) cudaEventDestroy(A->list_ev);
     if (A->astream) cudaStreamDestroy(A->astream);
     void* p[] = {A->U[0], A->U[1], A->phiG, A->phiF, A->iv, A->cslot, A->tgeo, A->tmeta, A->halo, A->inst_dt, A->inst_dtmin,
-                 A->inst_bc, A->stats, A->tiles, A->act, A->tile_r2, A->tile_bad, A->err, A->chunks, A->chunk_r2,
-                 A->chunk_bad};
+                 A->inst_bc, A->stats, A->tiles, A->act, A->tile_r2, A->tile_bad, A->err, A->queue, A->chunks,
+                 A->chunk_r2, A->chunk_bad};
     for (void* q : p) if (q) cudaFree(q);
     if (A->stream) cudaStreamDestroy(A->stream);
 }
@@ -523,10 +531,11 @@ int hcfd_arena_create(const hcfd_arena_params* prm, hcfd_arena** out) {
         (rc = dalloc(&h->inst_bc, p.max_instances)) || (rc = dalloc(&h->stats, p.max_instances)) ||
         (rc = dalloc(&h->tiles, 2 * h->tiles_cap)) || (rc = dalloc(&h->act, p.max_instances)) ||
         (rc = dalloc(&h->tile_r2, h->tiles_cap * (h->B / 32))) || (rc = dalloc(&h->tile_bad, h->tiles_cap * (h->B / 32))) ||
-        (rc = dalloc(&h->err, 1)) || (rc = dalloc(&h->chunks, h->chunks_cap)) ||
+        (rc = dalloc(&h->err, 1)) || (rc = dalloc(&h->queue, 1)) || (rc = dalloc(&h->chunks, h->chunks_cap)) ||
         (rc = dalloc(&h->chunk_r2, h->chunks_cap)) || (rc = dalloc(&h->chunk_bad, h->chunks_cap)))
         return bail(rc);
     cudaError_t ce = cudaMemsetAsync(h->err, 0, sizeof(unsigned int), h->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->queue, 0, sizeof(int), h->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->U[0], 0, 4 * ts * C, h->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->U[1], 0, 4 * ts * C, h->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(h->phiG, 0, 8 * ts * C, h->stream);
