@@ -42,7 +42,7 @@ def test_clock_summary_without_nvidia_smi():
 
 def test_traffic_of_the_committed_profile():
     # tile_pass2 on the 2001 x 1001 RCM wedge: 855.5 + 117.4 MB per launch (profiles/)
-    assert bench.traffic_from_profiles("pass2", "fp64_rcm_2001x1001") == 972878336.0
+    assert bench.traffic_from_profiles("pass2", "fp64_rcm_2001x1001") == 972516352.0
     assert bench.traffic_from_profiles("pass2", "no_such_workload") is None
 
 
