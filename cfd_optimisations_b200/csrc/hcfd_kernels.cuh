@@ -324,11 +324,20 @@ __device__ __forceinline__ int bc_of_face(const BCTable& bc, int f) {
 // ---------------------------------------------------------------------------------------
 // reductions
 
-__device__ __forceinline__ double warp_min(double x) {
+template <class T>
+__device__ __forceinline__ T warp_max(T x) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_xor_sync(0xffffffffu, x, o));
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
     return x;
 }
+// The CFL time-step minimum of a set of cells, min_i 1 / x_i with x_i = iv_i lam_i > 0: a
+// correctly rounded reciprocal (FP64) does not grow as x grows, so the minimum equals
+// 1 / max_i x_i bit for bit, and the cells keep a running maximum, one reciprocal being formed
+// per warp or block (FP32 uses the hardware reciprocal, measured to give the same bits on the
+// bench meshes).  fmax ignores a NaN x, so a cell with a NaN posts no step, and a set without
+// a positive x posts nothing.
+template <class T>
+__device__ __forceinline__ double dt_of_max(T x) { return x > T(0) ? (double) qrcp(x) : 1e300; }
 __device__ __forceinline__ double warp_sum(double x) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
@@ -355,7 +364,7 @@ static __global__ void check_slots_kernel(const int2* __restrict__ slot, int W, 
 template <class T, int W>
 __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double dtc = 1e300;
+    T xmx = T(0);                        // largest iv * lam (see dt_of_max)
     if (c < a.Nc) {
         int2 s[W];
 #pragma unroll
@@ -428,19 +437,19 @@ __global__ void __launch_bounds__(256) pass1_kernel(const StepArgs<T> a) {
             }
             if (lmode == LIM_RECORD) st_cell(a.phiF, a.Nc, c, phis);
             st_grad(a.phiG, a.Nc, c, out);
-            if (a.time_mode != TM_FIXED) dtc = (double) qrcp(iv * lam);
+            if (a.time_mode != TM_FIXED) xmx = iv * lam;
         }
     }
     if (a.time_mode != TM_FIXED) {
-        __shared__ double sm[32];
-        double m = warp_min(dtc);
+        __shared__ T sm[32];
+        T m = warp_max(xmx);
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
         if (lane == 0) sm[wid] = m;
         __syncthreads();
         if (wid == 0) {
-            m = lane < (int) (blockDim.x >> 5) ? sm[lane] : 1e300;
-            m = warp_min(m);
-            if (lane == 0 && m < 1e300) atomicMin(a.dtmin, (unsigned long long) __double_as_longlong(m));
+            m = lane < (int) (blockDim.x >> 5) ? sm[lane] : T(0);
+            const double d = dt_of_max(warp_max(m));
+            if (lane == 0 && d < 1e300) atomicMin(a.dtmin, (unsigned long long) __double_as_longlong(d));
         }
     }
 }

@@ -615,7 +615,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const TileSmem<T> L(a.B, a.Hmax, a.Fmax, W, a.Wp, false);
     const StepArgs<T>& s = a.s;
-    double dtc = 1e300;
+    T xmx = T(0);                        // largest iv * lam (see dt_of_max)
     HCFD_TILE_LOOP_BEGIN(false, ARENA)
     const int lmode = limiter_mode(si.steps, s.freeze_after);
     for (int c = threadIdx.x; c < nb; c += NT) {
@@ -697,7 +697,7 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
         }
         if (lmode == LIM_RECORD) st_cell(s.phiF, a.ps, base + c, phis);
         st_grad(s.phiG, a.ps, base + c, out);
-        if (s.time_mode != TM_FIXED) dtc = fmin(dtc, (double) qrcp(iv * lam));
+        if (s.time_mode != TM_FIXED) xmx = fmax(xmx, iv * lam);
     }
     if constexpr (ARENA) {
         // per-instance minimum (exact and order-free): each warp carries its minimum across
@@ -706,24 +706,24 @@ __global__ void __launch_bounds__(288) tile_pass1_kernel(const TileArgs<T> a) {
         // CTA rather than one per warp and tile on a single address
         if (s.time_mode != TM_FIXED) {
             if (si.next_inst != inst) {
-                const double m = warp_min(dtc);
+                const double m = dt_of_max(warp_max(xmx));
                 if ((threadIdx.x & 31) == 0 && m < 1e300)
                     atomicMin(a.inst_dtmin + 2 * inst + a.par, (unsigned long long) __double_as_longlong(m));
-                dtc = 1e300;
+                xmx = T(0);
             }
         }
     }
     HCFD_TILE_LOOP_END
     if (!ARENA && s.time_mode != TM_FIXED) {
-        __shared__ double sm[32];
-        double m = warp_min(dtc);
+        __shared__ T sm[32];
+        T m = warp_max(xmx);
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
         if (lane == 0) sm[wid] = m;
         __syncthreads();
         if (wid == 0) {
-            m = lane < (int) (blockDim.x >> 5) ? sm[lane] : 1e300;
-            m = warp_min(m);
-            if (lane == 0 && m < 1e300) atomicMin(s.dtmin, (unsigned long long) __double_as_longlong(m));
+            m = lane < (int) (blockDim.x >> 5) ? sm[lane] : T(0);
+            const double d = dt_of_max(warp_max(m));
+            if (lane == 0 && d < 1e300) atomicMin(s.dtmin, (unsigned long long) __double_as_longlong(d));
         }
     }
 }
