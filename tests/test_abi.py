@@ -4,6 +4,7 @@ import ctypes as ct
 import os
 import re
 import subprocess
+import sys
 
 import pytest
 
@@ -54,3 +55,21 @@ def test_no_gpu_here_means_a_cuda_error_not_a_fallback():
     with pytest.raises(H.HcfdError) as e:
         H.Solver(m)
     assert e.value.code == N.ECUDA
+
+
+def _lib_choice(value):
+    env = dict(os.environ, HCFD_LIB=value)
+    code = ("from cfd_optimisations_b200 import native as N; L = N.lib(); "
+            "print(N.LIB_PATH); print(L.hcfd_last_error())")
+    return subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, cwd=ROOT)
+
+
+def test_hcfd_lib_selects_the_checked_twin_and_rejects_other_values():
+    r = _lib_choice("checked")
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.splitlines()[0].endswith("libhcfd_gpu_checked.so")
+    r = _lib_choice("default")
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.splitlines()[0].endswith("libhcfd_gpu.so")
+    r = _lib_choice("fast")
+    assert r.returncode != 0 and "HCFD_LIB" in r.stderr
